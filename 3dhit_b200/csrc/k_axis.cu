@@ -1,0 +1,324 @@
+// Column FFT kernels along the strided spectral axes (x and y).
+//
+// A CTA owns one tile: all N positions along the transformed axis times W
+// contiguous z columns, for one value of the remaining axis.  Rows along the
+// axis are "compact" (see Geom): rows that are not stored are zeros on input
+// and dropped on output, so the dealiased path never moves the 5/9 of the
+// x/y frequencies the 2/3 rule removes.
+//
+// k_p1 and k_p3 are the x-axis ends of the RHS (src/hit3d/navierstokes.py:69-95):
+//   k_p1: curl (navierstokes.py:73-77) and the x part of to_physical for u and w;
+//   k_p3: x part of to_spectral, forcing (forcing.py:94-95,138-143), dealias +
+//         projection (grid.py:166-178), viscous term (navierstokes.py:95) and
+//         the RK4 stage algebra (integrators.py:32-38), then -- fused -- the
+//         next stage's k_p1 on the tile it just produced.
+#include <type_traits>
+
+#include "fft_core.cuh"
+#include "kernels.h"
+
+namespace hit {
+
+template <typename T, int N, int W, bool INV>
+__global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V2<T>* F = reinterpret_cast<V2<T>*>(smem_raw);
+  const int z0 = blockIdx.x * W;
+  const long long o = blockIdx.y, c = blockIdx.z;
+  const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
+  for (int e = threadIdx.x; e < N * W; e += NT) {
+    const int pos = e / W, col = e % W;
+    const int row = compact_row(pos, a.hin, a.Min, N);
+    V2<T> v = czero<T>();
+    if (row >= 0 && z0 + col < a.nz) v = src[(long long)row * a.s_a + col];
+    F[e] = v;
+  }
+  __syncthreads();
+  smem_fft<T, N, W, NT, W, 1, INV>(F, a.tw);
+  V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
+  for (int e = threadIdx.x; e < a.Mout * W; e += NT) {
+    const int row = e / W, col = e % W;
+    if (z0 + col < a.nz) dst[(long long)row * a.d_a + col] = F[full_pos(row, a.hout, a.Mout, N) * W + col];
+  }
+}
+
+// x-inverse of u and w = i k x u for one (ky row, z tile).  S holds the three
+// stage-input columns zero-padded to all N x positions; G is scratch.
+template <typename T, int N, int W>
+__device__ __forceinline__ void p1_body(V2<T>* S, V2<T>* G, int j, int z0, const Geom& g,
+                                        const KTab<T>& kt, const V2<T>* tw, V2<T>* t6,
+                                        long long t_c, long long t_x) {
+  const int fy = full_pos(j, g.hy, g.My, g.Ny);
+  const T ky = kt.ky[fy];
+  V2<T>* out = t6 + (long long)j * g.Mzp + z0;
+#pragma unroll 1
+  for (int q = 3; q < 6; ++q) {
+    for (int e = threadIdx.x; e < N * W; e += NT) {
+      const int pos = e / W, z = z0 + e % W;
+      const T kx = kt.kx[pos];
+      const T kz = z < g.Nzh ? kt.kz[z] : T(0);
+      const V2<T> u0 = S[e], u1 = S[N * W + e], u2 = S[2 * N * W + e];
+      V2<T> d;
+      if (q == 3) {
+        d.x = ky * u2.x - kz * u1.x;
+        d.y = ky * u2.y - kz * u1.y;
+      } else if (q == 4) {
+        d.x = kz * u0.x - kx * u2.x;
+        d.y = kz * u0.y - kx * u2.y;
+      } else {
+        d.x = kx * u1.x - ky * u0.x;
+        d.y = kx * u1.y - ky * u0.y;
+      }
+      G[e] = cmul_i(d);
+    }
+    __syncthreads();
+    smem_fft<T, N, W, NT, W, 1, true>(G, tw);
+    for (int e = threadIdx.x; e < N * W; e += NT)
+      out[q * t_c + (long long)(e / W) * t_x + e % W] = G[e];
+    __syncthreads();
+  }
+#pragma unroll 1
+  for (int q = 0; q < 3; ++q) {
+    V2<T>* Sq = S + q * N * W;
+    smem_fft<T, N, W, NT, W, 1, true>(Sq, tw);
+    for (int e = threadIdx.x; e < N * W; e += NT)
+      out[q * t_c + (long long)(e / W) * t_x + e % W] = Sq[e];
+  }
+}
+
+template <typename T, int N, int W>
+__global__ void __launch_bounds__(NT) k_p1(P1Args<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V2<T>* S = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* G = S + 3 * N * W;
+  const Geom& g = a.g;
+  const int j = blockIdx.y, z0 = blockIdx.x * W;
+  const V2<T>* src = a.s + (long long)j * g.Mzp + z0;
+  for (int c = 0; c < 3; ++c)
+    for (int e = threadIdx.x; e < N * W; e += NT) {
+      const int row = compact_row(e / W, g.hx, g.Mx, N);
+      S[c * N * W + e] = row >= 0 ? src[c * a.s_c + (long long)row * a.s_x + e % W] : czero<T>();
+    }
+  __syncthreads();
+  p1_body<T, N, W>(S, G, j, z0, g, a.k, a.tw, a.t6, a.t_c, a.t_x);
+}
+
+template <typename T, int N, int W>
+__global__ void __launch_bounds__(NT) k_p3(P3Args<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V2<T>* F = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* G = F + 3 * N * W;
+  __shared__ double red[32];
+  const Geom& g = a.g;
+  const int j = blockIdx.y, z0 = blockIdx.x * W;
+
+  const V2<T>* src = a.t3 + (long long)j * g.Mzp + z0;
+  for (int c = 0; c < 3; ++c)
+    for (int e = threadIdx.x; e < N * W; e += NT)
+      F[c * N * W + e] = src[c * a.t_c + (long long)(e / W) * a.t_x + e % W];
+  __syncthreads();
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) smem_fft<T, N, W, NT, W, 1, false>(F + c * N * W, a.tw);
+
+  const int fy = full_pos(j, g.hy, g.My, g.Ny);
+  const T ky = a.k.ky[fy];
+  const T cf = (a.forcing == 2 || a.forcing == 3) ? T(a.coef[0]) : T(0);
+  double sE = 0.0, sO = 0.0, sB = 0.0;
+  const long long cbase = (long long)j * g.Mzp + z0;
+  for (int e = threadIdx.x; e < g.Mx * W; e += NT) {
+    const int i = e / W, col = e % W, z = z0 + col;
+    const int pos = full_pos(i, g.hx, g.Mx, N);
+    V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
+    if (z < g.Mz) {
+      const long long idx = cbase + (long long)i * a.c_x + col;
+      const T kx = a.k.kx[pos], kz = a.k.kz[z];
+      const T k2 = k2_of(kx, ky, kz);
+      const T ik2 = inv_k2_of(k2);
+      const V2<T>* us_src = a.stage <= 1 ? a.u : a.s;
+      V2<T> us[3], du[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        us[c] = us_src[c * a.c_c + idx];
+        du[c] = F[c * N * W + pos * W + col];
+      }
+      // forcing term, added before dealias and projection (navierstokes.py:88-92)
+      if (a.forcing == 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], a.fA));
+      } else if (a.forcing == 2) {
+        if (a.kmin2 <= k2 && k2 <= a.kmax2) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], cf));
+        }
+      } else if (a.forcing == 3) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], cf));
+      }
+      if (!in_dealias(g, pos, fy, z)) {
+        du[0] = du[1] = du[2] = czero<T>();
+      }
+      // projection: div = (kx d0 + ky d1 + kz d2) / k^2 ; d -= k div
+      V2<T> div;
+      div.x = (kx * du[0].x + ky * du[1].x + kz * du[2].x) * ik2;
+      div.y = (kx * du[0].y + ky * du[1].y + kz * du[2].y) * ik2;
+      du[0] = csub(du[0], cscale(div, kx));
+      du[1] = csub(du[1], cscale(div, ky));
+      du[2] = csub(du[2], cscale(div, kz));
+      const T nk2 = a.nu * k2;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) du[c] = csub(du[c], cscale(us[c], nk2));
+
+      const long long o = idx;
+      switch (a.stage) {
+        case 0:
+#pragma unroll
+          for (int c = 0; c < 3; ++c) a.out[c * a.c_c + o] = du[c];
+          break;
+        case 1:
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            a.acc[c * a.c_c + o] = du[c];
+            ns[c] = cadd(us[c], cscale(du[c], a.a_next));
+            a.s[c * a.c_c + o] = ns[c];
+          }
+          break;
+        case 2:
+        case 3:
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            V2<T> ac = a.acc[c * a.c_c + o];
+            ac.x = ac.x + T(2) * du[c].x;
+            ac.y = ac.y + T(2) * du[c].y;
+            a.acc[c * a.c_c + o] = ac;
+            ns[c] = cadd(a.u[c * a.c_c + o], cscale(du[c], a.a_next));
+            a.s[c * a.c_c + o] = ns[c];
+          }
+          break;
+        default:
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const V2<T> ac = cadd(a.acc[c * a.c_c + o], du[c]);
+            ns[c] = cadd(a.u[c * a.c_c + o], cscale(ac, a.dt6));
+            a.u[c * a.c_c + o] = ns[c];
+          }
+          break;
+      }
+      if (a.partial) {
+        double a2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a2 += (double)ns[c].x * ns[c].x + (double)ns[c].y * ns[c].y;
+        const double w = herm_weight(g, z);
+        sE += w * a2;
+        sO += w * (double)k2 * a2;
+        if (a.kmin2 <= k2 && k2 <= a.kmax2) sB += w * a2;
+      }
+    }
+    if (a.fuse_p1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) F[c * N * W + pos * W + col] = ns[c];
+    }
+  }
+  if (a.fuse_p1) {
+    for (int e = threadIdx.x; e < N * W; e += NT)
+      if (compact_row(e / W, g.hx, g.Mx, N) < 0) F[e] = F[N * W + e] = F[2 * N * W + e] = czero<T>();
+  }
+  if (a.partial) {
+    const int b = blockIdx.y * gridDim.x + blockIdx.x;
+    double r = block_sum_f64(sE, red);
+    if (threadIdx.x == 0) a.partial[3 * b + 0] = r;
+    r = block_sum_f64(sO, red);
+    if (threadIdx.x == 0) a.partial[3 * b + 1] = r;
+    r = block_sum_f64(sB, red);
+    if (threadIdx.x == 0) a.partial[3 * b + 2] = r;
+  }
+  if (a.fuse_p1) {
+    __syncthreads();
+    p1_body<T, N, W>(F, G, j, z0, g, a.k, a.tw, a.t6, a.t6_c, a.t6_x);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+template <typename F> cudaError_t dispatch_len(int N, F&& f) {
+  switch (N) {
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 8: return f(std::integral_constant<int, 8>{});
+    case 16: return f(std::integral_constant<int, 16>{});
+    case 32: return f(std::integral_constant<int, 32>{});
+    case 64: return f(std::integral_constant<int, 64>{});
+    case 128: return f(std::integral_constant<int, 128>{});
+    case 256: return f(std::integral_constant<int, 256>{});
+    case 512: return f(std::integral_constant<int, 512>{});
+    case 1024: return f(std::integral_constant<int, 1024>{});
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T>
+cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, int nc, cudaStream_t st) {
+  return dispatch_len(N, [&](auto nn) {
+    constexpr int NN = decltype(nn)::value;
+    constexpr int W = tile_w<T>(NN);
+    const size_t smem = sizeof(V2<T>) * NN * W;
+    dim3 grid(nzt, no, nc);
+    if (inv) k_axis<T, NN, W, true><<<grid, NT, smem, st>>>(a);
+    else k_axis<T, NN, W, false><<<grid, NT, smem, st>>>(a);
+    return cudaGetLastError();
+  });
+}
+
+template <typename T> int p3_tile_w(int Nx) {
+  int w = 0;
+  dispatch_len(Nx, [&](auto nn) { w = tile_w<T>(decltype(nn)::value); return cudaSuccess; });
+  return w;
+}
+
+int p3_num_blocks(const Geom& g, int W) { return (g.Mzp / W) * g.My; }
+
+template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st) {
+  return dispatch_len(a.g.Nx, [&](auto nn) {
+    constexpr int NN = decltype(nn)::value;
+    constexpr int W = tile_w<T>(NN);
+    const size_t smem = sizeof(V2<T>) * 4 * NN * W;
+    dim3 grid(a.g.Mzp / W, a.g.My);
+    k_p1<T, NN, W><<<grid, NT, smem, st>>>(a);
+    return cudaGetLastError();
+  });
+}
+
+template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st) {
+  return dispatch_len(a.g.Nx, [&](auto nn) {
+    constexpr int NN = decltype(nn)::value;
+    constexpr int W = tile_w<T>(NN);
+    const size_t smem = sizeof(V2<T>) * 4 * NN * W;
+    dim3 grid(a.g.Mzp / W, a.g.My);
+    k_p3<T, NN, W><<<grid, NT, smem, st>>>(a);
+    return cudaGetLastError();
+  });
+}
+
+template <typename T> cudaError_t prepare_axis_kernels(int Nx) {
+  return dispatch_len(Nx, [&](auto nn) {
+    constexpr int NN = decltype(nn)::value;
+    constexpr int W = tile_w<T>(NN);
+    const int smem = (int)(sizeof(V2<T>) * 4 * NN * W);
+    cudaError_t e = cudaFuncSetAttribute(k_p1<T, NN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_p3<T, NN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  });
+}
+
+template cudaError_t launch_axis<float>(int, bool, const AxisArgs<float>&, int, int, int, cudaStream_t);
+template cudaError_t launch_axis<double>(int, bool, const AxisArgs<double>&, int, int, int, cudaStream_t);
+template cudaError_t launch_p1<float>(const P1Args<float>&, cudaStream_t);
+template cudaError_t launch_p1<double>(const P1Args<double>&, cudaStream_t);
+template cudaError_t launch_p3<float>(const P3Args<float>&, cudaStream_t);
+template cudaError_t launch_p3<double>(const P3Args<double>&, cudaStream_t);
+template cudaError_t prepare_axis_kernels<float>(int);
+template cudaError_t prepare_axis_kernels<double>(int);
+template int p3_tile_w<float>(int);
+template int p3_tile_w<double>(int);
+
+}  // namespace hit

@@ -1,0 +1,162 @@
+// Argument blocks and host launchers of the HIT3D kernels (internal header;
+// the public boundary is include/hit3d.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace hit {
+
+constexpr int NT = 256;  // threads per block of every FFT kernel
+
+// Columns (contiguous z entries) per x/y tile: one tile column block is at
+// most 32 KB, so P1/P3 (four tiles) fit in 128 KB of shared memory.
+template <typename T> constexpr int tile_w(int N) {
+  return (32768 / (N * (int)sizeof(V2<T>))) >= 8 ? 8 : (32768 / (N * (int)sizeof(V2<T>)));
+}
+
+// Plain column FFT along a strided axis ("a") of a 4-D array indexed
+// (comp, a, o, z): element at src + c*s_c + a*s_a + o*s_o + z.  Input rows
+// along a are compact (Min stored rows, hin non-negative), output rows compact
+// (Mout, hout); nz valid z columns.  grid = (ceil(nz/W), n_o, ncomp).
+template <typename T> struct AxisArgs {
+  const V2<T>* src;
+  V2<T>* dst;
+  long long s_c, s_a, s_o;
+  long long d_c, d_a, d_o;
+  int Min, hin, Mout, hout;
+  int nz;
+  const V2<T>* tw;
+};
+
+// P1: x-inverse of the stage input and of curl(u): 3 compact components in,
+// 6 x-physical components out (u_x,u_y,u_z, w_x,w_y,w_z).  grid = (Mzp/W, My).
+template <typename T> struct P1Args {
+  const V2<T>* s;   // (3, Mx, My, Mzp)
+  long long s_c, s_x;
+  V2<T>* t6;        // (6, Nx, My, Mzp)
+  long long t_c, t_x;
+  Geom g;
+  KTab<T> k;
+  const V2<T>* tw;
+};
+
+// P3: x-forward of the nonlinear term, RHS epilogue (forcing, dealias,
+// projection, viscous term), RK4 stage update, optional fused P1 of the new
+// stage input, optional per-block partial sums of the new stage input.
+template <typename T> struct P3Args {
+  const V2<T>* t3;  // (3, Nx, My, Mzp)
+  long long t_c, t_x;
+  V2<T>* u;         // state (3, Mx, My, Mzp)
+  V2<T>* acc;       // RK accumulator
+  V2<T>* s;         // stage input of stages 2..4
+  V2<T>* out;       // stage 0: du output
+  long long c_c, c_x;
+  V2<T>* t6;        // fused P1 output
+  long long t6_c, t6_x;
+  Geom g;
+  KTab<T> k;
+  const V2<T>* tw;
+  int stage;        // 0: rhs only (u_stage = u); 1..4: RK4 stage
+  int fuse_p1;
+  T nu, a_next, dt6;
+  int forcing;
+  T fA, kmin2, kmax2;
+  const double* coef;  // coef[0]: band c or hold-energy A (float64)
+  double* partial;     // per-block (3 per block) sums of the new stage input
+};
+
+// Fused z pass of the RHS: per (x, y) row, c2r of 6 components, u x w,
+// r2c of 3 components, in place (output = first 3 components).
+template <typename T> struct ZCrossArgs {
+  V2<T>* buf;  // (6, Nx, Ny, Mzp)
+  long long c_stride;
+  int nrows, Mz, Mzp;
+  T scale;     // 1/(Nx Ny Nz)
+  const V2<T>* tw;
+};
+
+// Plain z c2r / r2c for to_physical / to_spectral.
+template <typename T> struct ZRealArgs {
+  V2<T>* cbuf;        // complex rows, stride Mzp, Mz = Nz/2+1 valid
+  T* rbuf;            // real rows, stride Nz
+  long long cc_stride, rc_stride;  // per-component strides
+  int nrows, Mz, Mzp;
+  T scale;
+  const V2<T>* tw;
+};
+
+// Launchers (return cudaError_t of the launch).
+template <typename T> cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, int nc, cudaStream_t st);
+template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st);
+template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st);
+template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, cudaStream_t st);
+template <typename T> cudaError_t launch_zc2r(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st);
+template <typename T> cudaError_t launch_zr2c(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st);
+template <typename T> cudaError_t prepare_fft_kernels(int Nx, int Ny, int Nz);
+template <typename T> cudaError_t prepare_axis_kernels(int Nx);
+int p3_num_blocks(const Geom& g, int W);
+template <typename T> int p3_tile_w(int Nx);
+
+// ---- reductions / elementwise (k_reduce.cu) ----------------------------------
+// Scalar sums over modes: index 0: sum w|u|^2, 1: sum w k2 |u|^2, 2: band sum w|u|^2
+constexpr int NSCAL = 3;
+
+template <typename T> struct ModeSumArgs {
+  const V2<T>* u;        // 3 components
+  long long c_c, c_x, c_y;  // strides (comp, x-row, y-row)
+  Geom g;                // compact layout of u
+  KTab<T> k;
+  T kmin2, kmax2;        // band limits (squared, in the run dtype)
+  T k0;                  // shell width 2 pi / Lx in the run dtype
+  int nshell;            // smax + 1 bins (0 = no spectrum)
+  double* partial;       // [nblocks][3*nshell + NSCAL]
+};
+
+template <typename T> struct GatherArgs {
+  const V2<T>* ext;   // (3, Nx, Ny, Nzh)
+  V2<T>* cmp;         // (3, Mx, My, Mzp)
+  Geom g;
+  KTab<T> k;
+  T kmin2, kmax2;
+  double* partial;    // nullable: per-block NSCAL sums of the gathered state
+};
+
+template <typename T> cudaError_t launch_gather(const GatherArgs<T>& a, int nblocks, cudaStream_t st);
+template <typename T> cudaError_t launch_scatter(const V2<T>* cmp, V2<T>* ext, const Geom& g, cudaStream_t st);
+template <typename T> cudaError_t launch_check_box(const V2<T>* ext, const Geom& g, int* flag, cudaStream_t st);
+template <typename T> cudaError_t launch_dealias_project(const V2<T>* in, V2<T>* out, const Geom& g, KTab<T> k, int dd, int pp, cudaStream_t st);
+template <typename T> cudaError_t launch_mode_sums(const ModeSumArgs<T>& a, int nblocks, cudaStream_t st);
+template <typename T> cudaError_t launch_shell_scale(const V2<T>* in, V2<T>* out, const Geom& g, KTab<T> k, T k0, const double* c, int smax, cudaStream_t st);
+
+// Finalisers (deterministic, one pass over the per-block partials).
+struct CoefArgs {
+  const double* partial;
+  int nblocks;
+  int forcing;
+  double ntot2, nu, eps, E_target, tau, tiny;
+  double* coef;  // coef[0] = forcing coefficient, coef[1..3] = raw sums
+};
+cudaError_t launch_finalize_coef(const CoefArgs& a, cudaStream_t st);
+
+struct SumArgs {
+  const double* partial;
+  int nblocks, nvals;
+  double* sums;  // [nvals], Kahan-compensated block sums
+};
+cudaError_t launch_finalize_sums(const SumArgs& a, cudaStream_t st);
+
+struct BudgetArgs {
+  const double* sums;  // [3*nshell + NSCAL]
+  int nshell;
+  double* spec;        // nullable [nshell-1]   (shells 1..smax)
+  double* comp;        // nullable [3*(nshell-1)]
+  double* budget;      // nullable [4]: E, eps, P, Omega
+  int forcing;
+  double ntot2, nu, A, eps, E_target, tau, tiny;
+};
+cudaError_t launch_finalize_budget(const BudgetArgs& a, cudaStream_t st);
+
+}  // namespace hit

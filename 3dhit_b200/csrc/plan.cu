@@ -1,0 +1,760 @@
+// Plan object and C ABI (include/hit3d.h).
+//
+// A plan is made per grid (make_grid, src/hit3d/grid.py:89-132).  It owns the
+// wavenumber and twiddle tables and, per code path, the workspace of the
+// fused RHS:
+//   U, ACC, S, D  compact spectral state, RK accumulator, stage input, du
+//   T6            x-physical u and w (6 comps); its first 3 comps later hold
+//                 the y/z-forward products (T3)
+//   U6            x,y-physical u and w (6 comps); first 3 comps: z-forward u x w
+// One RHS evaluation (src/hit3d/navierstokes.py:69-95) is
+//   P1 (x-inverse, k_p1)  -> P2a (y-inverse)  -> P2b (z c2r, u x w, z r2c)
+//   -> P2c (y-forward)    -> P3 (x-forward + forcing/dealias/projection/
+//                              viscous/RK update + next stage's P1)
+// and one RK4 step (src/hit3d/integrators.py:32-38) is P1 plus four such
+// chains, captured once as a CUDA graph and replayed nsteps times (the
+// replacement for lax.scan in rollout, integrators.py:41-53).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include <algorithm>
+
+#include "fft_core.cuh"
+#include "hit3d.h"
+#include "kernels.h"
+
+using namespace hit;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(HIT_E_CUDA, std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define HIT_CK(expr)                                      \
+  do {                                                    \
+    cudaError_t _e = (expr);                              \
+    if (_e != cudaSuccess) return cuda_fail(_e, #expr);   \
+  } while (0)
+
+struct Buf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+int ensure(Buf& b, size_t bytes) {
+  if (b.bytes >= bytes) return HIT_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(HIT_E_ALLOC, "cudaMalloc(" + std::to_string(bytes) + " bytes) failed: " + cudaGetErrorString(e));
+  }
+  e = cudaMemset(b.p, 0, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemset(workspace)");
+  b.bytes = bytes;
+  return HIT_OK;
+}
+void release(Buf& b) {
+  if (b.p) cudaFree(b.p);
+  b = Buf{};
+}
+
+struct GraphKey {
+  double nu, A, eps, kmin, kmax, E_target, tau, dt;
+  int forcing;
+  bool operator==(const GraphKey& o) const {
+    return nu == o.nu && A == o.A && eps == o.eps && kmin == o.kmin && kmax == o.kmax && E_target == o.E_target &&
+           tau == o.tau && dt == o.dt && forcing == o.forcing;
+  }
+};
+
+struct Path {  // one code path: 0 = general (full layout), 1 = dealiased (2/3 box)
+  Geom g{};
+  bool ready = false;
+  Buf t6, u6, U, ACC, S, D, partial, coef;
+  int p3_blocks = 0, gather_blocks = 0;
+  cudaGraphExec_t exec = nullptr;
+  GraphKey key{};
+  bool key_valid = false;
+};
+
+Geom make_geom(int Nx, int Ny, int Nz, bool pruned) {
+  Geom g{};
+  g.Nx = Nx;
+  g.Ny = Ny;
+  g.Nz = Nz;
+  g.H = Nz / 2;
+  g.Nzh = Nz / 2 + 1;
+  g.cx = Nx / 3;
+  g.cy = Ny / 3;
+  g.cz = Nz / 3;
+  g.pruned = pruned ? 1 : 0;
+  if (pruned) {
+    g.Mx = 2 * g.cx + 1;
+    g.hx = g.cx + 1;
+    g.My = 2 * g.cy + 1;
+    g.hy = g.cy + 1;
+    g.Mz = g.cz + 1;
+  } else {
+    g.Mx = Nx;
+    g.hx = Nx / 2;
+    g.My = Ny;
+    g.hy = Ny / 2;
+    g.Mz = g.Nzh;
+  }
+  g.Mzp = (g.Mz + 7) / 8 * 8;
+  return g;
+}
+
+bool pow2_ok(int n) { return n >= 4 && n <= 1024 && (n & (n - 1)) == 0; }
+
+}  // namespace
+
+struct hit_plan {
+  int dtype = 0, Nx = 0, Ny = 0, Nz = 0;
+  double Lx = 0, Ly = 0, Lz = 0;
+  int device = 0;
+  int smax = 0;
+  Buf ktab, tw;
+  Path path[2];
+  Buf xws;                // to_physical / to_spectral workspace
+  Buf dpartial, dsums;    // diagnostics partials / sums
+  int diag_blocks = 0;
+  cudaStream_t cap = nullptr;  // private stream used only for graph capture
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+    else prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+template <typename T> KTab<T> ktab_of(const hit_plan* p) {
+  const T* base = static_cast<const T*>(p->ktab.p);
+  return KTab<T>{base, base + p->Nx, base + p->Nx + p->Ny};
+}
+template <typename T> const V2<T>* tw_of(const hit_plan* p) { return static_cast<const V2<T>*>(p->tw.p); }
+template <typename T> V2<T>* vp(const Buf& b) { return static_cast<V2<T>*>(b.p); }
+
+bool needs_coef(int forcing) { return forcing == HIT_FORCING_BAND || forcing == HIT_FORCING_HOLD_ENERGY; }
+
+template <typename T> int ensure_path(hit_plan* p, int which) {
+  Path& P = p->path[which];
+  if (P.ready) return HIT_OK;
+  P.g = make_geom(p->Nx, p->Ny, p->Nz, which == 1);
+  const Geom& g = P.g;
+  const size_t V = sizeof(V2<T>);
+  const size_t cmp = (size_t)3 * g.Mx * g.My * g.Mzp * V;
+  int rc;
+  if ((rc = ensure(P.t6, (size_t)6 * g.Nx * g.My * g.Mzp * V))) return rc;
+  if ((rc = ensure(P.u6, (size_t)6 * g.Nx * g.Ny * g.Mzp * V))) return rc;
+  if ((rc = ensure(P.U, cmp))) return rc;
+  if ((rc = ensure(P.ACC, cmp))) return rc;
+  if ((rc = ensure(P.S, cmp))) return rc;
+  if ((rc = ensure(P.D, cmp))) return rc;
+  const int W = p3_tile_w<T>(g.Nx);
+  P.p3_blocks = p3_num_blocks(g, W);
+  const long long nm = (long long)g.Mx * g.My * g.Mzp;
+  P.gather_blocks = (int)std::min<long long>((nm + NT - 1) / NT, 8 * 148);
+  const int nb = std::max(P.p3_blocks, P.gather_blocks);
+  if ((rc = ensure(P.partial, (size_t)3 * nb * sizeof(double)))) return rc;
+  if ((rc = ensure(P.coef, 8 * sizeof(double)))) return rc;
+  P.ready = true;
+  return HIT_OK;
+}
+
+struct Scalars {
+  int forcing;
+  double nu, A, eps, kmin2, kmax2, E_target, tau;
+};
+
+Scalars scalars_of(const hit_params* pr) {
+  Scalars s{};
+  s.forcing = pr->forcing_kind;
+  s.nu = pr->nu;
+  s.A = pr->A;
+  s.eps = pr->eps;
+  s.kmin2 = pr->kmin * pr->kmin;
+  s.kmax2 = pr->kmax * pr->kmax;
+  s.E_target = pr->E_target;
+  s.tau = pr->tau;
+  return s;
+}
+
+template <typename T> double tiny_of() { return sizeof(T) == 4 ? (double)FLT_EPSILON : DBL_EPSILON; }
+double ntot2_of(const hit_plan* p) {
+  const double n = (double)p->Nx * p->Ny * p->Nz;
+  return n * n;
+}
+
+template <typename T> int launch_coef(hit_plan* p, Path& P, const Scalars& s, int nblocks, cudaStream_t st) {
+  CoefArgs c{};
+  c.partial = static_cast<const double*>(P.partial.p);
+  c.nblocks = nblocks;
+  c.forcing = s.forcing;
+  c.ntot2 = ntot2_of(p);
+  c.nu = s.nu;
+  c.eps = s.eps;
+  c.E_target = s.E_target;
+  c.tau = s.tau;
+  c.tiny = tiny_of<T>();
+  c.coef = static_cast<double*>(P.coef.p);
+  HIT_CK(launch_finalize_coef(c, st));
+  return HIT_OK;
+}
+
+// reference layout -> compact U (+ forcing coefficient of the gathered state)
+template <typename T> int gather_state(hit_plan* p, Path& P, const void* u_hat, const Scalars& s, cudaStream_t st) {
+  GatherArgs<T> a{};
+  a.ext = static_cast<const V2<T>*>(u_hat);
+  a.cmp = vp<T>(P.U);
+  a.g = P.g;
+  a.k = ktab_of<T>(p);
+  a.kmin2 = (T)s.kmin2;
+  a.kmax2 = (T)s.kmax2;
+  a.partial = needs_coef(s.forcing) ? static_cast<double*>(P.partial.p) : nullptr;
+  HIT_CK(launch_gather<T>(a, P.gather_blocks, st));
+  if (needs_coef(s.forcing)) return launch_coef<T>(p, P, s, P.gather_blocks, st);
+  return HIT_OK;
+}
+
+template <typename T> int launch_p1_of(hit_plan* p, Path& P, const V2<T>* src, cudaStream_t st) {
+  const Geom& g = P.g;
+  P1Args<T> a{};
+  a.s = src;
+  a.s_c = (long long)g.Mx * g.My * g.Mzp;
+  a.s_x = (long long)g.My * g.Mzp;
+  a.t6 = vp<T>(P.t6);
+  a.t_c = (long long)g.Nx * g.My * g.Mzp;
+  a.t_x = (long long)g.My * g.Mzp;
+  a.g = g;
+  a.k = ktab_of<T>(p);
+  a.tw = tw_of<T>(p);
+  HIT_CK(launch_p1<T>(a, st));
+  return HIT_OK;
+}
+
+// P2a, P2b, P2c: T6 -> U6 (y-inverse), z pass in place on U6, U6[0:3] -> T6[0:3]
+template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st) {
+  const Geom& g = P.g;
+  const long long t6c = (long long)g.Nx * g.My * g.Mzp, u6c = (long long)g.Nx * g.Ny * g.Mzp;
+  const int Wy = p3_tile_w<T>(g.Ny);
+  AxisArgs<T> a{};
+  a.src = vp<T>(P.t6);
+  a.dst = vp<T>(P.u6);
+  a.s_c = t6c;
+  a.s_a = g.Mzp;
+  a.s_o = (long long)g.My * g.Mzp;
+  a.d_c = u6c;
+  a.d_a = g.Mzp;
+  a.d_o = (long long)g.Ny * g.Mzp;
+  a.Min = g.My;
+  a.hin = g.hy;
+  a.Mout = g.Ny;
+  a.hout = g.Ny / 2;
+  a.nz = g.Mzp;
+  a.tw = tw_of<T>(p);
+  HIT_CK(launch_axis<T>(g.Ny, true, a, g.Mzp / Wy, g.Nx, 6, st));
+
+  ZCrossArgs<T> z{};
+  z.buf = vp<T>(P.u6);
+  z.c_stride = u6c;
+  z.nrows = g.Nx * g.Ny;
+  z.Mz = g.Mz;
+  z.Mzp = g.Mzp;
+  z.scale = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
+  z.tw = tw_of<T>(p);
+  HIT_CK(launch_zcross<T>(g.H, z, st));
+
+  AxisArgs<T> b{};
+  b.src = vp<T>(P.u6);
+  b.dst = vp<T>(P.t6);
+  b.s_c = u6c;
+  b.s_a = g.Mzp;
+  b.s_o = (long long)g.Ny * g.Mzp;
+  b.d_c = t6c;
+  b.d_a = g.Mzp;
+  b.d_o = (long long)g.My * g.Mzp;
+  b.Min = g.Ny;
+  b.hin = g.Ny / 2;
+  b.Mout = g.My;
+  b.hout = g.hy;
+  b.nz = g.Mzp;
+  b.tw = tw_of<T>(p);
+  HIT_CK(launch_axis<T>(g.Ny, false, b, g.Mzp / Wy, g.Nx, 3, st));
+  return HIT_OK;
+}
+
+template <typename T>
+int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt, bool fuse, bool partial,
+                    cudaStream_t st) {
+  const Geom& g = P.g;
+  P3Args<T> a{};
+  a.t3 = vp<T>(P.t6);
+  a.t_c = (long long)g.Nx * g.My * g.Mzp;
+  a.t_x = (long long)g.My * g.Mzp;
+  a.u = vp<T>(P.U);
+  a.acc = vp<T>(P.ACC);
+  a.s = vp<T>(P.S);
+  a.out = vp<T>(P.D);
+  a.c_c = (long long)g.Mx * g.My * g.Mzp;
+  a.c_x = (long long)g.My * g.Mzp;
+  a.t6 = vp<T>(P.t6);
+  a.t6_c = a.t_c;
+  a.t6_x = a.t_x;
+  a.g = g;
+  a.k = ktab_of<T>(p);
+  a.tw = tw_of<T>(p);
+  a.stage = stage;
+  a.fuse_p1 = fuse ? 1 : 0;
+  a.nu = (T)s.nu;
+  a.a_next = stage == 3 ? (T)dt : (T)(0.5 * dt);
+  a.dt6 = (T)(dt / 6.0);
+  a.forcing = s.forcing;
+  a.fA = (T)s.A;
+  a.kmin2 = (T)s.kmin2;
+  a.kmax2 = (T)s.kmax2;
+  a.coef = static_cast<const double*>(P.coef.p);
+  a.partial = partial ? static_cast<double*>(P.partial.p) : nullptr;
+  HIT_CK(launch_p3<T>(a, st));
+  return HIT_OK;
+}
+
+// One RK4 step on the compact state U (P1 first, then four RHS chains).
+template <typename T> int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, cudaStream_t st) {
+  int rc;
+  const bool red = needs_coef(s.forcing);
+  if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
+  for (int stage = 1; stage <= 4; ++stage) {
+    if ((rc = launch_p2<T>(p, P, st))) return rc;
+    if ((rc = launch_p3_stage<T>(p, P, s, stage, dt, stage < 4, red, st))) return rc;
+    if (red && (rc = launch_coef<T>(p, P, s, P.p3_blocks, st))) return rc;
+  }
+  return HIT_OK;
+}
+
+int check_params(const hit_params* pr) {
+  if (!pr) return fail(HIT_E_INVALID, "params is NULL");
+  if (pr->forcing_kind < 0 || pr->forcing_kind > 3) return fail(HIT_E_INVALID, "unknown forcing_kind");
+  return HIT_OK;
+}
+
+template <typename T> int rhs_impl(hit_plan* p, const void* u_hat, const hit_params* pr, void* du, cudaStream_t st) {
+  int rc;
+  const int which = (pr->flags & HIT_FLAG_ASSUME_DEALIASED) ? 1 : 0;
+  if ((rc = ensure_path<T>(p, which))) return rc;
+  Path& P = p->path[which];
+  const Scalars s = scalars_of(pr);
+  if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
+  if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
+  if ((rc = launch_p2<T>(p, P, st))) return rc;
+  if ((rc = launch_p3_stage<T>(p, P, s, 0, 0.0, false, false, st))) return rc;
+  HIT_CK(launch_scatter<T>(vp<T>(P.D), static_cast<V2<T>*>(du), P.g, st));
+  return HIT_OK;
+}
+
+template <typename T>
+int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, void* out,
+                 cudaStream_t st) {
+  int rc;
+  const int which = (pr->flags & HIT_FLAG_ASSUME_DEALIASED) ? 1 : 0;
+  if ((rc = ensure_path<T>(p, which))) return rc;
+  Path& P = p->path[which];
+  const Scalars s = scalars_of(pr);
+  if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
+  if (nsteps > 0) {
+    const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing};
+    if (!P.exec || !P.key_valid || !(P.key == key)) {
+      if (P.exec) {
+        cudaGraphExecDestroy(P.exec);
+        P.exec = nullptr;
+      }
+      P.key_valid = false;
+      HIT_CK(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+      rc = enqueue_step<T>(p, P, s, dt, p->cap);
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamEndCapture(p->cap, &graph);
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+      e = cudaGraphInstantiate(&P.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+      P.key = key;
+      P.key_valid = true;
+    }
+    for (int64_t i = 0; i < nsteps; ++i) HIT_CK(cudaGraphLaunch(P.exec, st));
+  }
+  HIT_CK(launch_scatter<T>(vp<T>(P.U), static_cast<V2<T>*>(out), P.g, st));
+  return HIT_OK;
+}
+
+template <typename T> int to_physical_impl(hit_plan* p, const void* u_hat, int nc, void* u, cudaStream_t st) {
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  int rc;
+  if ((rc = ensure(p->xws, (size_t)nc * g.Nx * g.Ny * g.Mzp * sizeof(V2<T>)))) return rc;
+  const int Wx = p3_tile_w<T>(g.Nx), Wy = p3_tile_w<T>(g.Ny);
+  const long long wc = (long long)g.Nx * g.Ny * g.Mzp;
+  AxisArgs<T> a{};
+  a.src = static_cast<const V2<T>*>(u_hat);
+  a.dst = vp<T>(p->xws);
+  a.s_c = (long long)g.Nx * g.Ny * g.Nzh;
+  a.s_a = (long long)g.Ny * g.Nzh;
+  a.s_o = g.Nzh;
+  a.d_c = wc;
+  a.d_a = (long long)g.Ny * g.Mzp;
+  a.d_o = g.Mzp;
+  a.Min = a.Mout = g.Nx;
+  a.hin = a.hout = g.Nx / 2;
+  a.nz = g.Nzh;
+  a.tw = tw_of<T>(p);
+  HIT_CK(launch_axis<T>(g.Nx, true, a, (g.Nzh + Wx - 1) / Wx, g.Ny, nc, st));
+  AxisArgs<T> b{};
+  b.src = vp<T>(p->xws);
+  b.dst = vp<T>(p->xws);
+  b.s_c = b.d_c = wc;
+  b.s_a = b.d_a = g.Mzp;
+  b.s_o = b.d_o = (long long)g.Ny * g.Mzp;
+  b.Min = b.Mout = g.Ny;
+  b.hin = b.hout = g.Ny / 2;
+  b.nz = g.Nzh;
+  b.tw = tw_of<T>(p);
+  HIT_CK(launch_axis<T>(g.Ny, true, b, (g.Nzh + Wy - 1) / Wy, g.Nx, nc, st));
+  ZRealArgs<T> z{};
+  z.cbuf = vp<T>(p->xws);
+  z.rbuf = static_cast<T*>(u);
+  z.cc_stride = wc;
+  z.rc_stride = (long long)g.Nx * g.Ny * g.Nz;
+  z.nrows = g.Nx * g.Ny;
+  z.Mz = g.Nzh;
+  z.Mzp = g.Mzp;
+  z.scale = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
+  z.tw = tw_of<T>(p);
+  HIT_CK(launch_zc2r<T>(g.H, z, nc, st));
+  return HIT_OK;
+}
+
+template <typename T> int to_spectral_impl(hit_plan* p, const void* u, int nc, void* u_hat, cudaStream_t st) {
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  int rc;
+  if ((rc = ensure(p->xws, (size_t)nc * g.Nx * g.Ny * g.Mzp * sizeof(V2<T>)))) return rc;
+  const int Wx = p3_tile_w<T>(g.Nx), Wy = p3_tile_w<T>(g.Ny);
+  const long long wc = (long long)g.Nx * g.Ny * g.Mzp;
+  ZRealArgs<T> z{};
+  z.cbuf = vp<T>(p->xws);
+  z.rbuf = const_cast<T*>(static_cast<const T*>(u));
+  z.cc_stride = wc;
+  z.rc_stride = (long long)g.Nx * g.Ny * g.Nz;
+  z.nrows = g.Nx * g.Ny;
+  z.Mz = g.Nzh;
+  z.Mzp = g.Mzp;
+  z.scale = T(1);
+  z.tw = tw_of<T>(p);
+  HIT_CK(launch_zr2c<T>(g.H, z, nc, st));
+  AxisArgs<T> b{};
+  b.src = vp<T>(p->xws);
+  b.dst = vp<T>(p->xws);
+  b.s_c = b.d_c = wc;
+  b.s_a = b.d_a = g.Mzp;
+  b.s_o = b.d_o = (long long)g.Ny * g.Mzp;
+  b.Min = b.Mout = g.Ny;
+  b.hin = b.hout = g.Ny / 2;
+  b.nz = g.Nzh;
+  b.tw = tw_of<T>(p);
+  HIT_CK(launch_axis<T>(g.Ny, false, b, (g.Nzh + Wy - 1) / Wy, g.Nx, nc, st));
+  AxisArgs<T> a{};
+  a.src = vp<T>(p->xws);
+  a.dst = static_cast<V2<T>*>(u_hat);
+  a.s_c = wc;
+  a.s_a = (long long)g.Ny * g.Mzp;
+  a.s_o = g.Mzp;
+  a.d_c = (long long)g.Nx * g.Ny * g.Nzh;
+  a.d_a = (long long)g.Ny * g.Nzh;
+  a.d_o = g.Nzh;
+  a.Min = a.Mout = g.Nx;
+  a.hin = a.hout = g.Nx / 2;
+  a.nz = g.Nzh;
+  a.tw = tw_of<T>(p);
+  HIT_CK(launch_axis<T>(g.Nx, false, a, (g.Nzh + Wx - 1) / Wx, g.Ny, nc, st));
+  return HIT_OK;
+}
+
+// spectrum / budget over the reference layout
+template <typename T>
+int diag_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double* E, double* Ec, double* budget,
+              cudaStream_t st) {
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  const int nshell = (E || Ec) ? p->smax + 1 : 0;
+  const int nv = 3 * nshell + NSCAL;
+  int rc;
+  if ((rc = ensure(p->dpartial, (size_t)p->diag_blocks * nv * sizeof(double)))) return rc;
+  if ((rc = ensure(p->dsums, (size_t)nv * sizeof(double)))) return rc;
+  Scalars s{};
+  if (pr) s = scalars_of(pr);
+  ModeSumArgs<T> a{};
+  a.u = static_cast<const V2<T>*>(u_hat);
+  a.c_c = (long long)g.Nx * g.Ny * g.Nzh;
+  a.c_x = (long long)g.Ny * g.Nzh;
+  a.c_y = g.Nzh;
+  a.g = g;
+  a.k = ktab_of<T>(p);
+  a.kmin2 = (T)s.kmin2;
+  a.kmax2 = (T)s.kmax2;
+  a.k0 = (T)(2.0 * M_PI / p->Lx);
+  a.nshell = nshell;
+  a.partial = static_cast<double*>(p->dpartial.p);
+  HIT_CK(launch_mode_sums<T>(a, p->diag_blocks, st));
+  SumArgs sa{static_cast<const double*>(p->dpartial.p), p->diag_blocks, nv, static_cast<double*>(p->dsums.p)};
+  HIT_CK(launch_finalize_sums(sa, st));
+  BudgetArgs b{};
+  b.sums = static_cast<const double*>(p->dsums.p);
+  b.nshell = nshell;
+  b.spec = E;
+  b.comp = Ec;
+  b.budget = budget;
+  b.forcing = pr ? s.forcing : 0;
+  b.ntot2 = ntot2_of(p);
+  b.nu = s.nu;
+  b.A = s.A;
+  b.eps = s.eps;
+  b.E_target = s.E_target;
+  b.tau = s.tau;
+  b.tiny = tiny_of<T>();
+  HIT_CK(launch_finalize_budget(b, st));
+  return HIT_OK;
+}
+
+template <typename T> void fill_tables(hit_plan* p, std::string& kt, std::string& tw) {
+  const double two_pi = 2.0 * M_PI;
+  const int Nzh = p->Nz / 2 + 1;
+  kt.resize(sizeof(T) * (p->Nx + p->Ny + Nzh));
+  T* k = reinterpret_cast<T*>(&kt[0]);
+  auto freq = [](int i, int n) { return i < n / 2 ? i : i - n; };
+  for (int i = 0; i < p->Nx; ++i) k[i] = (T)(two_pi / p->Lx * (double)freq(i, p->Nx));
+  for (int i = 0; i < p->Ny; ++i) k[p->Nx + i] = (T)(two_pi / p->Ly * (double)freq(i, p->Ny));
+  for (int i = 0; i < Nzh; ++i) k[p->Nx + p->Ny + i] = (T)(two_pi / p->Lz * (double)i);
+  tw.resize(sizeof(V2<T>) * TWN);
+  V2<T>* w = reinterpret_cast<V2<T>*>(&tw[0]);
+  const long double pi = acosl(-1.0L);
+  for (int m = 0; m < TWN; ++m) {
+    const long double th = 2.0L * pi * (long double)m / (long double)TWN;
+    long double c = cosl(th), sn = -sinl(th);
+    if (fabsl(c) < 1e-30L) c = 0.0L;
+    if (fabsl(sn) < 1e-30L) sn = 0.0L;
+    w[m].x = (T)c;
+    w[m].y = (T)sn;
+  }
+}
+
+template <typename T> int create_impl(hit_plan* p) {
+  std::string kt, tw;
+  fill_tables<T>(p, kt, tw);
+  int rc;
+  if ((rc = ensure(p->ktab, kt.size()))) return rc;
+  if ((rc = ensure(p->tw, tw.size()))) return rc;
+  HIT_CK(cudaMemcpy(p->ktab.p, kt.data(), kt.size(), cudaMemcpyHostToDevice));
+  HIT_CK(cudaMemcpy(p->tw.p, tw.data(), tw.size(), cudaMemcpyHostToDevice));
+  HIT_CK(prepare_fft_kernels<T>(p->Nx, p->Ny, p->Nz));
+  return HIT_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+#define DISPATCH(p, call)                                   \
+  ((p)->dtype == HIT_DTYPE_F32 ? call<float> : call<double>)
+
+extern "C" {
+
+const char* hit_last_error_string(void) { return g_last_error.c_str(); }
+
+int hit_plan_create(int nx, int ny, int nz, double lx, double ly, double lz, int dtype, hit_plan** out) {
+  if (!out) return fail(HIT_E_INVALID, "out is NULL");
+  *out = nullptr;
+  if (!pow2_ok(nx) || !pow2_ok(ny) || !pow2_ok(nz))
+    return fail(HIT_E_UNSUPPORTED, "grid sizes must be powers of two in [4, 1024], got " + std::to_string(nx) + "x" +
+                                       std::to_string(ny) + "x" + std::to_string(nz));
+  if (dtype != HIT_DTYPE_F32 && dtype != HIT_DTYPE_F64) return fail(HIT_E_UNSUPPORTED, "dtype must be F32 or F64");
+  if (!(lx > 0) || !(ly > 0) || !(lz > 0)) return fail(HIT_E_INVALID, "box lengths must be positive");
+  hit_plan* p = new hit_plan();
+  p->dtype = dtype;
+  p->Nx = nx;
+  p->Ny = ny;
+  p->Nz = nz;
+  p->Lx = lx;
+  p->Ly = ly;
+  p->Lz = lz;
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e != cudaSuccess) {
+    delete p;
+    return cuda_fail(e, "cudaGetDevice");
+  }
+  const int nmax = std::max(nx, std::max(ny, nz));
+  p->smax = (int)std::ceil(std::sqrt(3.0) * nmax / 2.0) + 1;
+  const long long nm = (long long)nx * ny * (nz / 2 + 1);
+  p->diag_blocks = (int)std::min<long long>((nm + NT - 1) / NT, 8 * 148);
+  int rc = dtype == HIT_DTYPE_F32 ? create_impl<float>(p) : create_impl<double>(p);
+  if (rc == HIT_OK) {
+    e = cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreate");
+  }
+  if (rc != HIT_OK) {
+    hit_plan_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return HIT_OK;
+}
+
+int hit_plan_destroy(hit_plan* p) {
+  if (!p) return HIT_OK;
+  DeviceGuard dg(p->device);
+  for (Path& P : p->path) {
+    if (P.exec) cudaGraphExecDestroy(P.exec);
+    release(P.t6);
+    release(P.u6);
+    release(P.U);
+    release(P.ACC);
+    release(P.S);
+    release(P.D);
+    release(P.partial);
+    release(P.coef);
+  }
+  release(p->ktab);
+  release(p->tw);
+  release(p->xws);
+  release(p->dpartial);
+  release(p->dsums);
+  if (p->cap) cudaStreamDestroy(p->cap);
+  delete p;
+  return HIT_OK;
+}
+
+int hit_plan_num_shells(const hit_plan* p) { return p ? p->smax : 0; }
+
+int hit_to_physical(hit_plan* p, const void* u_hat, int nc, void* u, void* stream) {
+  if (!p || !u_hat || !u) return fail(HIT_E_INVALID, "NULL argument");
+  if (nc < 1 || nc > 6) return fail(HIT_E_INVALID, "ncomp must be in [1, 6]");
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, to_physical_impl)(p, u_hat, nc, u, (cudaStream_t)stream);
+}
+
+int hit_to_spectral(hit_plan* p, const void* u, int nc, void* u_hat, void* stream) {
+  if (!p || !u_hat || !u) return fail(HIT_E_INVALID, "NULL argument");
+  if (nc < 1 || nc > 6) return fail(HIT_E_INVALID, "ncomp must be in [1, 6]");
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, to_spectral_impl)(p, u, nc, u_hat, (cudaStream_t)stream);
+}
+
+int hit_dealias_project(hit_plan* p, const void* u_hat, int dd, int pp, void* out, void* stream) {
+  if (!p || !u_hat || !out) return fail(HIT_E_INVALID, "NULL argument");
+  DeviceGuard dg(p->device);
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  cudaError_t e;
+  if (p->dtype == HIT_DTYPE_F32)
+    e = launch_dealias_project<float>(static_cast<const float2*>(u_hat), static_cast<float2*>(out), g,
+                                      ktab_of<float>(p), dd, pp, (cudaStream_t)stream);
+  else
+    e = launch_dealias_project<double>(static_cast<const double2*>(u_hat), static_cast<double2*>(out), g,
+                                       ktab_of<double>(p), dd, pp, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "dealias_project");
+  return HIT_OK;
+}
+
+int hit_shell_scale(hit_plan* p, const void* u_hat, const double* c, void* out, void* stream) {
+  if (!p || !u_hat || !c || !out) return fail(HIT_E_INVALID, "NULL argument");
+  DeviceGuard dg(p->device);
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  const double k0 = 2.0 * M_PI / p->Lx;
+  cudaError_t e =
+      p->dtype == HIT_DTYPE_F32
+          ? launch_shell_scale<float>(static_cast<const float2*>(u_hat), static_cast<float2*>(out), g, ktab_of<float>(p),
+                                      (float)k0, c, p->smax, (cudaStream_t)stream)
+          : launch_shell_scale<double>(static_cast<const double2*>(u_hat), static_cast<double2*>(out), g,
+                                       ktab_of<double>(p), k0, c, p->smax, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "shell_scale");
+  return HIT_OK;
+}
+
+int hit_check_dealiased(hit_plan* p, const void* u_hat, int* flag, void* stream) {
+  if (!p || !u_hat || !flag) return fail(HIT_E_INVALID, "NULL argument");
+  DeviceGuard dg(p->device);
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, true);
+  cudaError_t e = p->dtype == HIT_DTYPE_F32
+                      ? launch_check_box<float>(static_cast<const float2*>(u_hat), g, flag, (cudaStream_t)stream)
+                      : launch_check_box<double>(static_cast<const double2*>(u_hat), g, flag, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "check_dealiased");
+  return HIT_OK;
+}
+
+int hit_rhs(hit_plan* p, const void* u_hat, const hit_params* pr, double t, void* du, void* stream) {
+  (void)t;  // no forcing of the reference depends on t
+  if (!p || !u_hat || !du) return fail(HIT_E_INVALID, "NULL argument");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, rhs_impl)(p, u_hat, pr, du, (cudaStream_t)stream);
+}
+
+int hit_rk4_step(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, double t, void* out, void* stream) {
+  (void)t;
+  if (!p || !u_hat || !out) return fail(HIT_E_INVALID, "NULL argument");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, 1, out, (cudaStream_t)stream);
+}
+
+int hit_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, double t0, void* out,
+                void* stream) {
+  (void)t0;
+  if (!p || !u_hat || !out) return fail(HIT_E_INVALID, "NULL argument");
+  if (nsteps < 0) return fail(HIT_E_INVALID, "nsteps must be >= 0");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, nsteps, out, (cudaStream_t)stream);
+}
+
+int hit_energy_spectrum(hit_plan* p, const void* u_hat, double* E, double* Ec, void* stream) {
+  if (!p || !u_hat) return fail(HIT_E_INVALID, "NULL argument");
+  if (!E && !Ec) return fail(HIT_E_INVALID, "no output requested");
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, diag_impl)(p, u_hat, nullptr, E, Ec, nullptr, (cudaStream_t)stream);
+}
+
+int hit_energy_budget(hit_plan* p, const void* u_hat, const hit_params* pr, double* out, void* stream) {
+  if (!p || !u_hat || !out) return fail(HIT_E_INVALID, "NULL argument");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, diag_impl)(p, u_hat, pr, nullptr, nullptr, out, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+/*
+ * hit3d.h -- C ABI of the B200-native HIT3D pseudo-spectral Navier-Stokes
+ * hot path (sm_100a kernels in 3dhit_b200/csrc).
+ *
+ * Every entry point replaces one pure function of the reference JAX package
+ * (nfrank22-gh/3DHIT, src/hit3d).  The spectral state is the reference's
+ * layout: one complex array (ncomp, Nx, Ny, Nz/2+1), C order, components
+ * first, rfft-halved axis last (src/hit3d/grid.py:7-14).  complex64 for
+ * HIT_DTYPE_F32, complex128 for HIT_DTYPE_F64; physical fields are real
+ * (ncomp, Nx, Ny, Nz).
+ *
+ * Conventions
+ *  - All array arguments are DEVICE pointers owned by the caller; inputs are
+ *    never modified (the reference functions are pure).  Output buffers may
+ *    not alias inputs.
+ *  - `stream` is a cudaStream_t passed as void*; every call is asynchronous
+ *    on it.  A plan is bound to one stream at a time and is not re-entrant;
+ *    separate plans are independent.
+ *  - Workspace belongs to the plan.  It is allocated on first use of a
+ *    code path (dealiased or general, see HIT_FLAG_ASSUME_DEALIASED) and then
+ *    reused, so steady-state calls allocate nothing.
+ *  - Return value: HIT_OK or a negative HIT_E* status; hit_last_error_string
+ *    gives the message of the last failure on the calling thread.
+ *  - Sizes: every N_i a power of two, 4 <= N_i <= 1024.
+ */
+#ifndef HIT3D_B200_H
+#define HIT3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HIT_OK 0
+#define HIT_E_INVALID (-1)     /* bad argument (shape, pointer, kind)        */
+#define HIT_E_CUDA (-2)        /* a CUDA runtime call failed                  */
+#define HIT_E_ALLOC (-3)       /* device allocation failed                    */
+#define HIT_E_NONFINITE (-4)   /* non-finite value met by a checked reduction */
+#define HIT_E_UNSUPPORTED (-5) /* size or dtype outside the supported set     */
+
+#define HIT_DTYPE_F32 0
+#define HIT_DTYPE_F64 1
+
+/* Forcing plug-ins (src/hit3d/forcing.py:55-163) plus the energy-holding
+ * Lundgren variant, which has no reference counterpart. */
+#define HIT_FORCING_NONE 0        /* NoForcing      forcing.py:55-71          */
+#define HIT_FORCING_LINEAR 1      /* LinearForcing  forcing.py:74-106 (f=A u) */
+#define HIT_FORCING_BAND 2        /* BandForcing    forcing.py:109-163        */
+#define HIT_FORCING_HOLD_ENERGY 3 /* A = (2 nu Omega - (E-E_target)/tau)/(2E) */
+
+/* Flags (hit_params.flags). */
+#define HIT_FLAG_ASSUME_DEALIASED 1u /* input is zero outside the 2/3 box: the
+                                        transforms skip those modes           */
+
+typedef struct hit_plan hit_plan;
+
+/* Differentiable scalars of the RHS: NSParams (src/hit3d/navierstokes.py:40-59)
+ * and the forcing coefficients that are pytree leaves in the reference. */
+typedef struct hit_params {
+  double nu;         /* kinematic viscosity                                  */
+  int forcing_kind;  /* HIT_FORCING_*                                        */
+  unsigned flags;    /* HIT_FLAG_*                                           */
+  double A;          /* LINEAR: coefficient                                  */
+  double eps;        /* BAND: injection rate                                 */
+  double kmin, kmax; /* BAND: shell limits |k| in [kmin, kmax]               */
+  double E_target;   /* HOLD_ENERGY: held kinetic energy                     */
+  double tau;        /* HOLD_ENERGY: relaxation time (<=0 or inf: none)      */
+} hit_params;
+
+/* make_grid (src/hit3d/grid.py:89-132): plan for an Nx x Ny x Nz box of
+ * lengths Lx, Ly, Lz in the given dtype on the current CUDA device. */
+int hit_plan_create(int nx, int ny, int nz, double lx, double ly, double lz,
+                    int dtype, hit_plan **out);
+int hit_plan_destroy(hit_plan *plan);
+
+/* Number of shells returned by the spectrum calls:
+ * smax = ceil(sqrt(3) max(N)/2) + 1 (src/hit3d/diagnostics.py:76-82). */
+int hit_plan_num_shells(const hit_plan *plan);
+
+/* to_physical (src/hit3d/grid.py:181-183): irfftn of ncomp components,
+ * (ncomp,Nx,Ny,Nz/2+1) complex -> (ncomp,Nx,Ny,Nz) real.  1 <= ncomp <= 6. */
+int hit_to_physical(hit_plan *plan, const void *u_hat, int ncomp, void *u,
+                    void *stream);
+
+/* to_spectral (src/hit3d/grid.py:186-188): unnormalised rfftn. */
+int hit_to_spectral(hit_plan *plan, const void *u, int ncomp, void *u_hat,
+                    void *stream);
+
+/* dealias then project (src/hit3d/grid.py:166-178); either step can be
+ * switched off (do_dealias / do_project = 0).  3 components. */
+int hit_dealias_project(hit_plan *plan, const void *u_hat, int do_dealias,
+                        int do_project, void *out, void *stream);
+
+/* Per-shell rescale used by random_field (src/hit3d/fields.py:51-68):
+ * out = u_hat * c[shell(k)] for 3 components, shell(k) = floor(|k|/k0 + 0.5)
+ * as in the reference; c_dev is a DEVICE double array of
+ * hit_plan_num_shells()+1 factors indexed by shell 0..smax (larger shells
+ * clamp to smax, like jnp indexing). */
+int hit_shell_scale(hit_plan *plan, const void *u_hat, const double *c_dev,
+                    void *out, void *stream);
+
+/* Writes 1 to *flag_dev (a device int) if u_hat has a nonzero mode outside
+ * the 2/3 box, else 0.  Used to choose HIT_FLAG_ASSUME_DEALIASED. */
+int hit_check_dealiased(hit_plan *plan, const void *u_hat, int *flag_dev,
+                        void *stream);
+
+/* rhs(u_hat, params, t) of make_ns_rhs (src/hit3d/navierstokes.py:62-97). */
+int hit_rhs(hit_plan *plan, const void *u_hat, const hit_params *params,
+            double t, void *du_hat, void *stream);
+
+/* rk4_step (src/hit3d/integrators.py:32-38). */
+int hit_rk4_step(hit_plan *plan, const void *u_hat, const hit_params *params,
+                 double dt, double t, void *out, void *stream);
+
+/* rollout (src/hit3d/integrators.py:41-53): nsteps RK4 steps, replayed from a
+ * CUDA graph of one step; no host synchronisation inside. */
+int hit_rollout(hit_plan *plan, const void *u_hat, const hit_params *params,
+                double dt, int64_t nsteps, double t0, void *out, void *stream);
+
+/* energy_spectrum / component_spectra (src/hit3d/diagnostics.py:94-114),
+ * accumulated in float64 (Kahan-compensated across blocks).  E_dev and
+ * Ecomp_dev are DEVICE double arrays of hit_plan_num_shells() and
+ * 3*hit_plan_num_shells() entries (either may be NULL); entry s is shell s+1. */
+int hit_energy_spectrum(hit_plan *plan, const void *u_hat, double *E_dev,
+                        double *Ecomp_dev, void *stream);
+
+/* energy_budget (src/hit3d/diagnostics.py:162-172) in float64:
+ * out_dev[0] = E, [1] = eps = 2 nu Omega, [2] = P (forcing injection),
+ * [3] = Omega.  out_dev is a DEVICE double[4]. */
+int hit_energy_budget(hit_plan *plan, const void *u_hat,
+                      const hit_params *params, double *out_dev, void *stream);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *hit_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HIT3D_B200_H */
