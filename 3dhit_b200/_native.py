@@ -32,6 +32,8 @@ HIT_FORCING_BAND = 2
 HIT_FORCING_HOLD_ENERGY = 3
 
 HIT_FLAG_ASSUME_DEALIASED = 1
+HIT_NUM_KERNEL_CLASSES = 6
+KERNEL_CLASSES = ("x-inverse", "y-inverse", "z-pass", "y-forward", "x-forward+epilogue", "forcing-coef")
 
 # Every entry point of include/hit3d.h: name -> (restype, argtypes)
 _vp, _i, _d, _i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64
@@ -67,6 +69,7 @@ SIGNATURES = {
     "hit_rhs": (_i, [_vp, _vp, _PP, _d, _vp, _vp]),
     "hit_rk4_step": (_i, [_vp, _vp, _PP, _d, _d, _vp, _vp]),
     "hit_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _d, _vp, _vp]),
+    "hit_profile_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _vp, _vp, _vp, _vp]),
     "hit_energy_spectrum": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "hit_energy_budget": (_i, [_vp, _vp, _PP, _vp, _vp]),
     "hit_last_error_string": (ctypes.c_char_p, []),

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include <algorithm>
 
@@ -41,6 +42,8 @@ int fail(int code, const std::string& msg) {
 int cuda_fail(cudaError_t e, const char* where) {
   return fail(HIT_E_CUDA, std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
 }
+
+int ck(cudaError_t e, const char* where) { return e == cudaSuccess ? HIT_OK : cuda_fail(e, where); }
 
 #define HIT_CK(expr)                                      \
   do {                                                    \
@@ -202,6 +205,38 @@ Scalars scalars_of(const hit_params* pr) {
   return s;
 }
 
+// Optional per-launch event timer (hit_profile_rollout).
+struct Prof {
+  cudaStream_t st = nullptr;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> cls;
+  int begin() { return mark(); }
+  int end(int c) {
+    cls.push_back(c);
+    return mark();
+  }
+  int mark() {
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreate(&e);
+    if (r != cudaSuccess) return cuda_fail(r, "cudaEventCreate");
+    ev.push_back(e);
+    r = cudaEventRecord(e, st);
+    if (r != cudaSuccess) return cuda_fail(r, "cudaEventRecord");
+    return HIT_OK;
+  }
+  ~Prof() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+};
+
+#define TIMED(pf, c, expr)                   \
+  do {                                       \
+    int _r;                                  \
+    if ((pf) && (_r = (pf)->begin())) return _r; \
+    if ((_r = (expr))) return _r;            \
+    if ((pf) && (_r = (pf)->end(c))) return _r;  \
+  } while (0)
+
 template <typename T> double tiny_of() { return sizeof(T) == 4 ? (double)FLT_EPSILON : DBL_EPSILON; }
 double ntot2_of(const hit_plan* p) {
   const double n = (double)p->Nx * p->Ny * p->Nz;
@@ -256,7 +291,7 @@ template <typename T> int launch_p1_of(hit_plan* p, Path& P, const V2<T>* src, c
 }
 
 // P2a, P2b, P2c: T6 -> U6 (y-inverse), z pass in place on U6, U6[0:3] -> T6[0:3]
-template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st) {
+template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st, Prof* pf = nullptr) {
   const Geom& g = P.g;
   const long long t6c = (long long)g.Nx * g.My * g.Mzp, u6c = (long long)g.Nx * g.Ny * g.Mzp;
   const int Wy = p3_tile_w<T>(g.Ny);
@@ -275,7 +310,7 @@ template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st) {
   a.hout = g.Ny / 2;
   a.nz = g.Mzp;
   a.tw = tw_of<T>(p);
-  HIT_CK(launch_axis<T>(g.Ny, true, a, g.Mzp / Wy, g.Nx, 6, st));
+  TIMED(pf, 1, ck(launch_axis<T>(g.Ny, true, a, g.Mzp / Wy, g.Nx, 6, st), "y-inverse"));
 
   ZCrossArgs<T> z{};
   z.buf = vp<T>(P.u6);
@@ -285,7 +320,7 @@ template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st) {
   z.Mzp = g.Mzp;
   z.scale = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
   z.tw = tw_of<T>(p);
-  HIT_CK(launch_zcross<T>(g.H, z, st));
+  TIMED(pf, 2, ck(launch_zcross<T>(g.H, z, st), "z pass"));
 
   AxisArgs<T> b{};
   b.src = vp<T>(P.u6);
@@ -302,7 +337,7 @@ template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st) {
   b.hout = g.hy;
   b.nz = g.Mzp;
   b.tw = tw_of<T>(p);
-  HIT_CK(launch_axis<T>(g.Ny, false, b, g.Mzp / Wy, g.Nx, 3, st));
+  TIMED(pf, 3, ck(launch_axis<T>(g.Ny, false, b, g.Mzp / Wy, g.Nx, 3, st), "y-forward"));
   return HIT_OK;
 }
 
@@ -342,14 +377,43 @@ int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt
 }
 
 // One RK4 step on the compact state U (P1 first, then four RHS chains).
-template <typename T> int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, cudaStream_t st) {
+template <typename T>
+int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, cudaStream_t st, Prof* pf = nullptr) {
   int rc;
   const bool red = needs_coef(s.forcing);
-  if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
+  TIMED(pf, 0, launch_p1_of<T>(p, P, vp<T>(P.U), st));
   for (int stage = 1; stage <= 4; ++stage) {
-    if ((rc = launch_p2<T>(p, P, st))) return rc;
-    if ((rc = launch_p3_stage<T>(p, P, s, stage, dt, stage < 4, red, st))) return rc;
-    if (red && (rc = launch_coef<T>(p, P, s, P.p3_blocks, st))) return rc;
+    if ((rc = launch_p2<T>(p, P, st, pf))) return rc;
+    TIMED(pf, 4, launch_p3_stage<T>(p, P, s, stage, dt, stage < 4, red, st));
+    if (red) TIMED(pf, 5, launch_coef<T>(p, P, s, P.p3_blocks, st));
+  }
+  return HIT_OK;
+}
+
+template <typename T>
+int profile_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, void* out,
+                 double* ms, int* launches, cudaStream_t st) {
+  int rc;
+  const int which = (pr->flags & HIT_FLAG_ASSUME_DEALIASED) ? 1 : 0;
+  if ((rc = ensure_path<T>(p, which))) return rc;
+  Path& P = p->path[which];
+  const Scalars s = scalars_of(pr);
+  if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
+  Prof pf;
+  pf.st = st;
+  for (int64_t i = 0; i < nsteps; ++i)
+    if ((rc = enqueue_step<T>(p, P, s, dt, st, &pf))) return rc;
+  HIT_CK(launch_scatter<T>(vp<T>(P.U), static_cast<V2<T>*>(out), P.g, st));
+  HIT_CK(cudaStreamSynchronize(st));
+  for (int c = 0; c < HIT_NUM_KERNEL_CLASSES; ++c) {
+    ms[c] = 0.0;
+    launches[c] = 0;
+  }
+  for (size_t k = 0; k < pf.cls.size(); ++k) {
+    float t = 0.f;
+    HIT_CK(cudaEventElapsedTime(&t, pf.ev[2 * k], pf.ev[2 * k + 1]));
+    ms[pf.cls[k]] += t;
+    launches[pf.cls[k]] += 1;
   }
   return HIT_OK;
 }
@@ -740,6 +804,16 @@ int hit_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, double dt,
   if ((rc = check_params(pr))) return rc;
   DeviceGuard dg(p->device);
   return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, nsteps, out, (cudaStream_t)stream);
+}
+
+int hit_profile_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, void* out,
+                        double* ms, int* launches, void* stream) {
+  if (!p || !u_hat || !out || !ms || !launches) return fail(HIT_E_INVALID, "NULL argument");
+  if (nsteps < 1) return fail(HIT_E_INVALID, "nsteps must be >= 1");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, profile_impl)(p, u_hat, pr, dt, nsteps, out, ms, launches, (cudaStream_t)stream);
 }
 
 int hit_energy_spectrum(hit_plan* p, const void* u_hat, double* E, double* Ec, void* stream) {

@@ -24,6 +24,15 @@ from .navierstokes import NSRHS, resolve_flags
 __all__ = ["rk4_step", "rollout", "evolve"]
 
 
+def _as_tensor(rhs, u_hat):
+    if isinstance(u_hat, torch.Tensor):
+        return u_hat
+    g = getattr(rhs, "grid", None)
+    if g is not None:
+        return _check_state(u_hat, g)
+    return torch.as_tensor(u_hat, device="cuda")
+
+
 def _fused(rhs, params):
     return isinstance(rhs, NSRHS) and native_params(params.nu, params.forcing) is not None
 
@@ -38,6 +47,7 @@ def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None):
         nat.call("hit_rk4_step", g.plan.handle, nat.ptr(u_hat), p, float(dt), float(t), nat.ptr(out),
                  nat.stream_ptr(g.device))
         return out
+    u_hat = _as_tensor(rhs, u_hat)
     k1 = rhs(u_hat, params, t)
     k2 = rhs(u_hat + 0.5 * dt * k1, params, t + 0.5 * dt)
     k3 = rhs(u_hat + 0.5 * dt * k2, params, t + 0.5 * dt)

@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark: RK4 steps/s of band-forced HIT at 512^3 in float32 on B200.
+
+Workload (one "step" = one RK4 step of the full RHS, 4 fused RHS chains):
+  512^3 grid, L = 2 pi, float32 state (3, 512, 512, 257) complex64;
+  BandForcing(eps=0.1, kmin=1, kmax=2), nu = 6e-4, dt from CFL 0.5 of the
+  initial field (held constant); initial field: seeded random-phase
+  solenoidal field with the Rosales-Meneveau k^4 exp(-2 (k/4)^2) spectrum
+  rescaled to u_rms = 1, generated on the device.
+Timing: W untimed warm-up steps, then K steps replayed from the CUDA graph,
+  bracketed by barrier + synchronize, CUDA events on the launching stream,
+  max over ranks.  The state and workspace (~6 GB) are far larger than L2,
+  so no explicit flush is needed.  One process per GPU; ranks are independent
+  replicas (the path does not shard), value = all ranks' steps / max time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "RK4 steps/s @512³ fp32 (1 B200, %HBM roofline)"
+WORKLOAD = "band-forced HIT 512^3 fp32 (BandForcing eps=0.1 k=[1,2], nu=6e-4, CFL 0.5), RK4 rollout"
+NU, EPS, KMIN, KMAX, CFL = 6e-4, 0.1, 1.0, 2.0, 0.5
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def spectral_bytes(N, itemsize=8):
+    """S(N) = N*N*(N/2+1) complex elements of one component."""
+    return N * N * (N // 2 + 1) * itemsize
+
+
+def kernel_alg_bytes(N, itemsize=8):
+    """Algorithmic bytes per launch of each kernel class on the dealiased path
+    (compact extents, padding excluded): what the kernel must read + write."""
+    c = N // 3
+    M, Mz = 2 * c + 1, c + 1
+    A = M * M * Mz          # compact spectral modes
+    Bx = N * M * Mz         # x-physical, (ky, kz) in the box
+    Cx = N * N * Mz         # x,y-physical, kz in the box
+    p3 = 3 * Bx + (51 * A + 18 * Bx) / 4.0  # mean over the 4 stages
+    return {
+        "x-inverse": (3 * A + 6 * Bx) * itemsize,
+        "y-inverse": (6 * Bx + 6 * Cx) * itemsize,
+        "z-pass": (6 * Cx + 3 * Cx) * itemsize,
+        "y-forward": (3 * Cx + 3 * Bx) * itemsize,
+        "x-forward+epilogue": p3 * itemsize,
+        "forcing-coef": 0.0,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_baseline(N, orc, seed=0):
+    """One RK4 step of the same workload on the host cores with the CPU oracle
+    (NumPy/SciPy restatement of the reference, float32, scipy.fft with all
+    cores)."""
+    cores = os.cpu_count() or 1
+    orc.set_workers(cores)
+    g = orc.make_grid(N, dtype=np.float32)
+    rng = np.random.default_rng(seed)
+    # a dealiased solenoidal field with the same spectrum shape (host IC)
+    u = orc.hit_initial_field(seed, g) if N <= 256 else _cheap_ic(orc, g, rng)
+    p = orc.NSParams(nu=NU, forcing=orc.BandForcing(eps=EPS, kmin=KMIN, kmax=KMAX))
+    rhs = orc.make_ns_rhs(g)
+    dt = 1e-4
+    t0 = time.perf_counter()
+    orc.rk4_step(rhs, u, p, dt, 0.0)
+    t = time.perf_counter() - t0
+    return {"value": 1.0 / t, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"1 RK4 step at {N}^3 fp32 of the same band-forced RHS by the CPU oracle "
+                      f"(NumPy/SciPy restatement of the reference, scipy.fft workers={cores}); {t:.1f} s"}
+
+
+def _cheap_ic(orc, g, rng):
+    """Random dealiased, projected spectral state (skips the per-shell rescale
+    of the full IC, which only shapes the spectrum)."""
+    shape = (3, g.Nx, g.Ny, g.Nz // 2 + 1)
+    u = (rng.standard_normal(shape, dtype=np.float32) + 1j * rng.standard_normal(shape, dtype=np.float32))
+    u = orc.project(orc.dealias(u.astype(np.complex64), g), g)
+    k2 = g.k2
+    return (u * np.exp(-k2 / 32.0).astype(np.float32) * np.float32(1e-3)).astype(np.complex64)
+
+
+def run_reference(args):
+    """--impl reference: the CPU implementation of the path timed on the host
+    cores (the oracle port; the JAX reference cannot be installed here)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import hit3d_oracle as orc
+    N = args.size
+    cores = os.cpu_count() or 1
+    orc.set_workers(cores)
+    g = orc.make_grid(N, dtype=np.float32)
+    u = _cheap_ic(orc, g, np.random.default_rng(0)) if N > 256 else orc.hit_initial_field(0, g)
+    p = orc.NSParams(nu=NU, forcing=orc.BandForcing(eps=EPS, kmin=KMIN, kmax=KMAX))
+    rhs = orc.make_ns_rhs(g)
+    dt = 1e-4
+    warm = min(args.warmup, 1)
+    steps = max(1, min(args.steps, 2))
+    for _ in range(warm):
+        u = orc.rk4_step(rhs, u, p, dt, 0.0)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u = orc.rk4_step(rhs, u, p, dt, 0.0)
+    t = time.perf_counter() - t0
+    v = steps / t
+    sample = (f"{steps} timed RK4 steps (after {warm} warm-up) at {N}^3 fp32 by the CPU oracle "
+              f"(NumPy/SciPy restatement of the reference hot path; scipy.fft workers={cores})")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1000 * t / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": N},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    h3 = importlib.import_module("3dhit_b200")
+    nat = importlib.import_module("3dhit_b200._native")
+    N = args.size
+    g = h3.make_grid(N, dtype=torch.float32, device=dev)
+    u0 = h3.hit_initial_field(rank, g)
+    dt = h3.cfl_dt(u0, g, CFL)
+    p = h3.NSParams(nu=NU, forcing=h3.BandForcing(eps=EPS, kmin=KMIN, kmax=KMAX))
+    rhs = h3.make_ns_rhs(g)
+    assert h3.is_dealiased(u0, g)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (captures the step graph)
+    u = h3.rollout(rhs, u0, p, dt, args.warmup, assume_dealiased=True)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K graph-replayed steps ------------------------------
+    clocks = ClockSampler(local) if rank == 0 else None
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    u = h3.rollout(rhs, u, p, dt, args.steps, assume_dealiased=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ck = clocks.stop() if clocks else None
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    E_end = float(h3.energy(u, g))
+    if not np.isfinite(E_end):
+        raise RuntimeError("non-finite energy after the timed rollout")
+    ms_step = ms_max / args.steps
+    value = world * args.steps / (ms_max / 1000.0)
+    launches_per_step = 1 + 4 * 5  # x-inverse, then 4 x (y-inv, z, y-fwd, x-fwd+epi, coef)
+
+    # ---- per-kernel device times (events around every launch) -------------
+    import ctypes
+    msa = (ctypes.c_double * nat.HIT_NUM_KERNEL_CLASSES)()
+    cnt = (ctypes.c_int * nat.HIT_NUM_KERNEL_CLASSES)()
+    out = torch.empty_like(u)
+    prm = h3.forcing.native_params(NU, p.forcing, nat.HIT_FLAG_ASSUME_DEALIASED)
+    nat.call("hit_profile_rollout", g.plan.handle, nat.ptr(u), prm, float(dt), args.profile_steps,
+             nat.ptr(out), msa, cnt, nat.stream_ptr(dev))
+    alg = kernel_alg_bytes(N)
+    per_kernel = {}
+    for i, name in enumerate(nat.KERNEL_CLASSES):
+        if cnt[i]:
+            avg = msa[i] / cnt[i]
+            per_kernel[name] = {"launches": cnt[i], "total_ms": msa[i], "avg_ms": avg,
+                                "alg_bytes": alg[name],
+                                "alg_gbs": alg[name] / (avg / 1000.0) / 1e9 if alg[name] else None}
+    tot = sum(v["total_ms"] for v in per_kernel.values())
+    for v in per_kernel.values():
+        v["share"] = v["total_ms"] / tot
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["total_ms"])
+    peak, peak_kind = peaks()
+    traffic = None
+    try:
+        with open(os.path.join(REPO, "profiles", "dram_traffic_512.json")) as f:
+            traffic = json.load(f).get(dom)
+    except Exception:
+        pass
+    dk = per_kernel[dom]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": dk["alg_gbs"], "peak": peak, "unit": "GB/s",
+                "frac": dk["alg_gbs"] / peak, "traffic": traffic,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                "alg_bytes_per_launch": dk["alg_bytes"], "avg_launch_ms": dk["avg_ms"]}
+    S = spectral_bytes(N)
+    step_model = {"model": "127*S(N) bytes per RK4 step", "bytes_per_step": 127 * S,
+                  "achieved_gbs": 127 * S / (ms_step / 1000.0) / 1e9,
+                  "frac": 127 * S / (ms_step / 1000.0) / 1e9 / peak,
+                  "alg_bytes_per_step_pruned": sum(v["alg_bytes"] * v["launches"] for v in per_kernel.values())
+                  / args.profile_steps}
+
+    # ---- end to end through the public API with host buffers ---------------
+    e2e = None
+    if not args.no_e2e:
+        host_in = u0.cpu().pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        h3.rollout(rhs, host_in.to(dev, non_blocking=True), p, dt, 1)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        ud = host_in.to(dev, non_blocking=True)
+        ur = h3.rollout(rhs, ud, p, dt, args.steps)  # public call: path check included
+        host_out.copy_(ur, non_blocking=True)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([a0.elapsed_time(a1)], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        nb = host_in.numel() * host_in.element_size()
+        e2e = {"value": world * args.steps / (float(te.item()) / 1000.0), "unit": "steps/s",
+               "h2d_bytes_per_step": nb / args.steps, "d2h_bytes_per_step": nb / args.steps,
+               "note": f"one public rollout({args.steps} steps) call from pinned host state to pinned host result",
+               "wall_s": time.perf_counter() - t0}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import hit3d_oracle as orc
+        cpu = cpu_baseline(N, orc)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": N, "dt": dt, "nu": NU,
+                       "l2": "inputs larger than L2 (state + workspace ~6 GB per GPU)",
+                       "parallelism": f"replicas x{world}", "path": "dealiased (2/3-box transforms)"},
+            "grid_point_steps_per_s": value * N**3,
+            "roofline": roofline, "step_roofline": step_model, "kernels": per_kernel,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+            "clocks": ck, "energy_end": E_end,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

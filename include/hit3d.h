@@ -118,6 +118,20 @@ int hit_rk4_step(hit_plan *plan, const void *u_hat, const hit_params *params,
 int hit_rollout(hit_plan *plan, const void *u_hat, const hit_params *params,
                 double dt, int64_t nsteps, double t0, void *out, void *stream);
 
+/* Measurement hook (no reference counterpart): the same nsteps RK4 steps as
+ * hit_rollout, launched one kernel at a time with a CUDA event pair around
+ * every launch on `stream`.  Host arrays ms_out / launches_out of
+ * HIT_NUM_KERNEL_CLASSES entries receive, per kernel class, the summed device
+ * time in ms and the number of launches.  Classes: 0 x-inverse (P1),
+ * 1 y-inverse, 2 z pass (c2r, u x w, r2c), 3 y-forward, 4 x-forward + RHS/RK4
+ * epilogue (+ next stage's x-inverse), 5 forcing coefficient.  Synchronises
+ * `stream` before returning. */
+#define HIT_NUM_KERNEL_CLASSES 6
+int hit_profile_rollout(hit_plan *plan, const void *u_hat,
+                        const hit_params *params, double dt, int64_t nsteps,
+                        void *out, double *ms_out, int *launches_out,
+                        void *stream);
+
 /* energy_spectrum / component_spectra (src/hit3d/diagnostics.py:94-114),
  * accumulated in float64 (Kahan-compensated across blocks).  E_dev and
  * Ecomp_dev are DEVICE double arrays of hit_plan_num_shells() and
