@@ -72,6 +72,7 @@ SIGNATURES = {
     "hit_profile_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _vp, _vp, _vp, _vp]),
     "hit_energy_spectrum": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "hit_energy_budget": (_i, [_vp, _vp, _PP, _vp, _vp]),
+    "hit_energy_spectrum_noalloc": (_i, [_i, _i, _i, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "hit_last_error_string": (ctypes.c_char_p, []),
 }
 

@@ -647,6 +647,11 @@ template <typename T> int create_impl(hit_plan* p) {
 
 }  // namespace
 
+namespace hit {
+// Sets the thread's last-error string for entry points defined in other files.
+int record_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace hit
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------

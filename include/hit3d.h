@@ -145,6 +145,23 @@ int hit_energy_spectrum(hit_plan *plan, const void *u_hat, double *E_dev,
 int hit_energy_budget(hit_plan *plan, const void *u_hat,
                       const hit_params *params, double *out_dev, void *stream);
 
+/* energy_spectrum without any device allocation.  No counterpart in the
+ * reference: it serves callers that cannot allocate device memory -- code
+ * running while its stream is being captured into a CUDA graph, an XLA custom
+ * call that must take every buffer from XLA, a process whose device memory is
+ * already reserved by another allocator.  Same outputs as hit_energy_spectrum
+ * (E_dev: smax doubles, Ecomp_dev: 3*smax doubles, device pointers, either may
+ * be NULL) for a grid given by its sizes, lengths and dtype; no plan is needed.
+ * The per-block partial sums live in a fixed 4 MiB static device array held by
+ * every GPU that loads this library until exit.  The first call on a device
+ * (with that device current) looks up that array's address; make it before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be ordered by the caller.  Grids are limited to powers of
+ * two in [4, 1024] per axis; larger sizes are rejected with HIT_E_UNSUPPORTED. */
+int hit_energy_spectrum_noalloc(int nx, int ny, int nz, double lx, double ly,
+                                double lz, int dtype, const void *u_hat,
+                                double *E_dev, double *Ecomp_dev, void *stream);
+
 /* Message of the last failed call on this thread ("" if none). */
 const char *hit_last_error_string(void);
 
