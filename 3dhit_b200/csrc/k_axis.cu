@@ -4,7 +4,10 @@
 // contiguous z columns, for one value of the remaining axis.  Rows along the
 // axis are "compact" (see Geom): rows that are not stored are zeros on input
 // and dropped on output, so the dealiased path never moves the 5/9 of the
-// x/y frequencies the 2/3 rule removes.
+// x/y frequencies the 2/3 rule removes.  The first FFT stage reads straight
+// from global memory (or from the fused prologue) and the last stage writes
+// straight to global memory (or to the fused epilogue); only the middle stages
+// go through shared memory.
 //
 // k_p1 and k_p3 are the x-axis ends of the RHS (src/hit3d/navierstokes.py:69-95):
 //   k_p1: curl (navierstokes.py:73-77) and the x part of to_physical for u and w;
@@ -20,112 +23,121 @@
 namespace hit {
 
 template <typename T, int N, int W, bool INV>
-__global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a) {
+__global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V2<T>* F = reinterpret_cast<V2<T>*>(smem_raw);
-  const int z0 = blockIdx.x * W;
-  const long long o = blockIdx.y, c = blockIdx.z;
-  const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
-  for (int e = threadIdx.x; e < N * W; e += NT) {
-    const int pos = e / W, col = e % W;
-    const int row = compact_row(pos, a.hin, a.Min, N);
-    V2<T> v = czero<T>();
-    if (row >= 0 && z0 + col < a.nz) v = src[(long long)row * a.s_a + col];
-    F[e] = v;
-  }
+  V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* B = A + N * W;
+  V2<T>* tws = B + N * W;
+  fill_stage_twiddles<T, N, false, NT>(tws, a.tw);
   __syncthreads();
-  smem_fft<T, N, W, NT, W, 1, INV>(F, a.tw);
-  V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
-  for (int e = threadIdx.x; e < a.Mout * W; e += NT) {
-    const int row = e / W, col = e % W;
-    if (z0 + col < a.nz) dst[(long long)row * a.d_a + col] = F[full_pos(row, a.hout, a.Mout, N) * W + col];
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int zt = tile % nzt, rest = tile / nzt;
+    const int z0 = zt * W;
+    const long long o = rest % no, c = rest / no;
+    const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
+    V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
+    const bool zc = z0 + W <= a.nz;  // whole tile inside the valid columns
+    fft_io<T, N, W, NT, W, 1, INV>(
+        A, B, tws,
+        [&](int pos, int col) {
+          const int row = compact_row(pos, a.hin, a.Min, N);
+          return (row >= 0 && (zc || z0 + col < a.nz)) ? src[(long long)row * a.s_a + col] : czero<T>();
+        },
+        [&](int pos, int col, V2<T> v) {
+          const int row = compact_row(pos, a.hout, a.Mout, N);
+          if (row >= 0 && (zc || z0 + col < a.nz)) dst[(long long)row * a.d_a + col] = v;
+        });
+    __syncthreads();  // the next tile's first stage rewrites A
   }
 }
 
 // x-inverse of u and w = i k x u for one (ky row, z tile).  S holds the three
-// stage-input columns zero-padded to all N x positions; G is scratch.
+// stage-input columns in compact rows (Mx x W each); A/B are the FFT buffers.
 template <typename T, int N, int W>
-__device__ __forceinline__ void p1_body(V2<T>* S, V2<T>* G, int j, int z0, const Geom& g,
-                                        const KTab<T>& kt, const V2<T>* tw, V2<T>* t6,
-                                        long long t_c, long long t_x) {
+__device__ __forceinline__ void p1_body(const V2<T>* S, V2<T>* A, V2<T>* B, int j, int z0, const Geom& g,
+                                        const KTab<T>& kt, const V2<T>* tws, V2<T>* t6, long long t_c,
+                                        long long t_x) {
   const int fy = full_pos(j, g.hy, g.My, g.Ny);
   const T ky = kt.ky[fy];
   V2<T>* out = t6 + (long long)j * g.Mzp + z0;
+  const int MW = g.Mx * W;
 #pragma unroll 1
-  for (int q = 3; q < 6; ++q) {
-    for (int e = threadIdx.x; e < N * W; e += NT) {
-      const int pos = e / W, z = z0 + e % W;
-      const T kx = kt.kx[pos];
-      const T kz = z < g.Nzh ? kt.kz[z] : T(0);
-      const V2<T> u0 = S[e], u1 = S[N * W + e], u2 = S[2 * N * W + e];
-      V2<T> d;
-      if (q == 3) {
-        d.x = ky * u2.x - kz * u1.x;
-        d.y = ky * u2.y - kz * u1.y;
-      } else if (q == 4) {
-        d.x = kz * u0.x - kx * u2.x;
-        d.y = kz * u0.y - kx * u2.y;
-      } else {
-        d.x = kx * u1.x - ky * u0.x;
-        d.y = kx * u1.y - ky * u0.y;
-      }
-      G[e] = cmul_i(d);
-    }
-    __syncthreads();
-    smem_fft<T, N, W, NT, W, 1, true>(G, tw);
-    for (int e = threadIdx.x; e < N * W; e += NT)
-      out[q * t_c + (long long)(e / W) * t_x + e % W] = G[e];
-    __syncthreads();
-  }
-#pragma unroll 1
-  for (int q = 0; q < 3; ++q) {
-    V2<T>* Sq = S + q * N * W;
-    smem_fft<T, N, W, NT, W, 1, true>(Sq, tw);
-    for (int e = threadIdx.x; e < N * W; e += NT)
-      out[q * t_c + (long long)(e / W) * t_x + e % W] = Sq[e];
+  for (int q = 0; q < 6; ++q) {
+    fft_io<T, N, W, NTP, W, 1, true>(
+        A, B, tws,
+        [&](int pos, int col) {
+          const int row = compact_row(pos, g.hx, g.Mx, N);
+          if (row < 0) return czero<T>();
+          const int e = row * W + col;
+          if (q < 3) return S[q * MW + e];
+          const int z = z0 + col;
+          const T kx = kt.kx[pos];
+          const T kz = z < g.Nzh ? kt.kz[z] : T(0);
+          const V2<T> u0 = S[e], u1 = S[MW + e], u2 = S[2 * MW + e];
+          V2<T> d;
+          if (q == 3) {
+            d.x = ky * u2.x - kz * u1.x;
+            d.y = ky * u2.y - kz * u1.y;
+          } else if (q == 4) {
+            d.x = kz * u0.x - kx * u2.x;
+            d.y = kz * u0.y - kx * u2.y;
+          } else {
+            d.x = kx * u1.x - ky * u0.x;
+            d.y = kx * u1.y - ky * u0.y;
+          }
+          return cmul_i(d);
+        },
+        [&](int pos, int col, V2<T> v) { out[q * t_c + (long long)pos * t_x + col] = v; });
+    __syncthreads();  // the next transform's first stage rewrites A
   }
 }
 
 template <typename T, int N, int W>
-__global__ void __launch_bounds__(NT) k_p1(P1Args<T> a) {
+__global__ void __launch_bounds__(NTP) k_p1(P1Args<T> a, int nzt, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  V2<T>* S = reinterpret_cast<V2<T>*>(smem_raw);
-  V2<T>* G = S + 3 * N * W;
   const Geom& g = a.g;
-  const int j = blockIdx.y, z0 = blockIdx.x * W;
-  const V2<T>* src = a.s + (long long)j * g.Mzp + z0;
-  for (int c = 0; c < 3; ++c)
-    for (int e = threadIdx.x; e < N * W; e += NT) {
-      const int row = compact_row(e / W, g.hx, g.Mx, N);
-      S[c * N * W + e] = row >= 0 ? src[c * a.s_c + (long long)row * a.s_x + e % W] : czero<T>();
+  V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* B = A + N * W;
+  V2<T>* tws = B + N * W;
+  V2<T>* S = tws + tw_size<false>(N);  // 3 x Mx x W
+  fill_stage_twiddles<T, N, false, NTP>(tws, a.tw);
+  const int MW = g.Mx * W;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int j = tile / nzt, z0 = (tile % nzt) * W;
+    const V2<T>* src = a.s + (long long)j * g.Mzp + z0;
+    for (int e = threadIdx.x; e < 3 * MW; e += NTP) {
+      const int c = e / MW, r = e - c * MW;
+      S[e] = src[c * a.s_c + (long long)(r / W) * a.s_x + r % W];
     }
-  __syncthreads();
-  p1_body<T, N, W>(S, G, j, z0, g, a.k, a.tw, a.t6, a.t_c, a.t_x);
+    __syncthreads();
+    p1_body<T, N, W>(S, A, B, j, z0, g, a.k, tws, a.t6, a.t_c, a.t_x);
+  }
 }
 
 template <typename T, int N, int W>
-__global__ void __launch_bounds__(NT) k_p3(P3Args<T> a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V2<T>* F = reinterpret_cast<V2<T>*>(smem_raw);
-  V2<T>* G = F + 3 * N * W;
-  __shared__ double red[32];
+__device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, const V2<T>* tws, V2<T>* F, double* red,
+                                        int j, int z0, int tile) {
   const Geom& g = a.g;
-  const int j = blockIdx.y, z0 = blockIdx.x * W;
+  const int MW = g.Mx * W;
 
   const V2<T>* src = a.t3 + (long long)j * g.Mzp + z0;
-  for (int c = 0; c < 3; ++c)
-    for (int e = threadIdx.x; e < N * W; e += NT)
-      F[c * N * W + e] = src[c * a.t_c + (long long)(e / W) * a.t_x + e % W];
-  __syncthreads();
 #pragma unroll 1
-  for (int c = 0; c < 3; ++c) smem_fft<T, N, W, NT, W, 1, false>(F + c * N * W, a.tw);
+  for (int c = 0; c < 3; ++c) {
+    fft_io<T, N, W, NTP, W, 1, false>(
+        A, B, tws, [&](int pos, int col) { return src[c * a.t_c + (long long)pos * a.t_x + col]; },
+        [&](int pos, int col, V2<T> v) {
+          const int row = compact_row(pos, g.hx, g.Mx, N);
+          if (row >= 0) F[c * MW + row * W + col] = v;
+        });
+    __syncthreads();
+  }
 
   const int fy = full_pos(j, g.hy, g.My, g.Ny);
   const T ky = a.k.ky[fy];
   const T cf = (a.forcing == 2 || a.forcing == 3) ? T(a.coef[0]) : T(0);
   double sE = 0.0, sO = 0.0, sB = 0.0;
   const long long cbase = (long long)j * g.Mzp + z0;
-  for (int e = threadIdx.x; e < g.Mx * W; e += NT) {
+  for (int e = threadIdx.x; e < MW; e += NTP) {
     const int i = e / W, col = e % W, z = z0 + col;
     const int pos = full_pos(i, g.hx, g.Mx, N);
     V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
@@ -139,7 +151,7 @@ __global__ void __launch_bounds__(NT) k_p3(P3Args<T> a) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         us[c] = us_src[c * a.c_c + idx];
-        du[c] = F[c * N * W + pos * W + col];
+        du[c] = F[c * MW + e];
       }
       // forcing term, added before dealias and projection (navierstokes.py:88-92)
       if (a.forcing == 1) {
@@ -215,15 +227,11 @@ __global__ void __launch_bounds__(NT) k_p3(P3Args<T> a) {
     }
     if (a.fuse_p1) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) F[c * N * W + pos * W + col] = ns[c];
+      for (int c = 0; c < 3; ++c) F[c * MW + e] = ns[c];
     }
   }
-  if (a.fuse_p1) {
-    for (int e = threadIdx.x; e < N * W; e += NT)
-      if (compact_row(e / W, g.hx, g.Mx, N) < 0) F[e] = F[N * W + e] = F[2 * N * W + e] = czero<T>();
-  }
   if (a.partial) {
-    const int b = blockIdx.y * gridDim.x + blockIdx.x;
+    const int b = tile;
     double r = block_sum_f64(sE, red);
     if (threadIdx.x == 0) a.partial[3 * b + 0] = r;
     r = block_sum_f64(sO, red);
@@ -231,9 +239,23 @@ __global__ void __launch_bounds__(NT) k_p3(P3Args<T> a) {
     r = block_sum_f64(sB, red);
     if (threadIdx.x == 0) a.partial[3 * b + 2] = r;
   }
-  if (a.fuse_p1) {
-    __syncthreads();
-    p1_body<T, N, W>(F, G, j, z0, g, a.k, a.tw, a.t6, a.t6_c, a.t6_x);
+  __syncthreads();  // F complete; A/B free for the next tile or the fused x-inverse
+  if (a.fuse_p1) p1_body<T, N, W>(F, A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x);
+}
+
+template <typename T, int N, int W>
+__global__ void __launch_bounds__(NTP) k_p3(P3Args<T> a, int nzt, int ntiles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* B = A + N * W;
+  V2<T>* tws = B + N * W;
+  V2<T>* F = tws + tw_size<false>(N);  // 3 x Mx x W: nl, then the new stage input
+  fill_stage_twiddles<T, N, false, NTP>(tws, a.tw);
+  __syncthreads();
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int j = tile / nzt, z0 = (tile % nzt) * W;
+    p3_tile<T, N, W>(a, A, B, tws, F, red, j, z0, tile);
   }
 }
 
@@ -256,22 +278,39 @@ template <typename F> cudaError_t dispatch_len(int N, F&& f) {
   }
 }
 
+// P1/P3 shared memory: A, B (N x W each) and the 3 compact tiles (Mx x W).
+template <typename T, int N> size_t p_smem(int W, int Mx) {
+  return sizeof(V2<T>) * ((size_t)(2 * N + 3 * Mx) * W + tw_size<false>(N));
+}
+template <typename T, int N, int W> constexpr size_t axis_smem() { return sizeof(V2<T>) * (2 * N * W + tw_size<false>(N)); }
+
 template <typename T>
 cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, int nc, cudaStream_t st) {
   return dispatch_len(N, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
     constexpr int W = tile_w<T>(NN);
-    const size_t smem = sizeof(V2<T>) * NN * W;
-    dim3 grid(nzt, no, nc);
-    if (inv) k_axis<T, NN, W, true><<<grid, NT, smem, st>>>(a);
-    else k_axis<T, NN, W, false><<<grid, NT, smem, st>>>(a);
+    const size_t smem = axis_smem<T, NN, W>();
+    const long long ntiles = (long long)nzt * no * nc;
+    static int c_inv = 0, c_fwd = 0;
+    if (inv)
+      k_axis<T, NN, W, true><<<resident_grid(k_axis<T, NN, W, true>, NT, smem, ntiles, c_inv), NT, smem, st>>>(
+          a, nzt, no, (int)ntiles);
+    else
+      k_axis<T, NN, W, false><<<resident_grid(k_axis<T, NN, W, false>, NT, smem, ntiles, c_fwd), NT, smem, st>>>(
+          a, nzt, no, (int)ntiles);
     return cudaGetLastError();
   });
 }
 
 template <typename T> int p3_tile_w(int Nx) {
   int w = 0;
-  dispatch_len(Nx, [&](auto nn) { w = tile_w<T>(decltype(nn)::value); return cudaSuccess; });
+  dispatch_len(Nx, [&](auto nn) { w = tile_wp<T>(decltype(nn)::value); return cudaSuccess; });
+  return w;
+}
+
+template <typename T> int axis_tile_w(int N) {
+  int w = 0;
+  dispatch_len(N, [&](auto nn) { w = tile_w<T>(decltype(nn)::value); return cudaSuccess; });
   return w;
 }
 
@@ -280,10 +319,12 @@ int p3_num_blocks(const Geom& g, int W) { return (g.Mzp / W) * g.My; }
 template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st) {
   return dispatch_len(a.g.Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
-    constexpr int W = tile_w<T>(NN);
-    const size_t smem = sizeof(V2<T>) * 4 * NN * W;
-    dim3 grid(a.g.Mzp / W, a.g.My);
-    k_p1<T, NN, W><<<grid, NT, smem, st>>>(a);
+    constexpr int W = tile_wp<T>(NN);
+    const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
+    const size_t smem = p_smem<T, NN>(W, a.g.Mx);
+    static int cache = 0;
+    k_p1<T, NN, W><<<resident_grid(k_p1<T, NN, W>, NTP, p_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
+        a, nzt, ntiles);
     return cudaGetLastError();
   });
 }
@@ -291,22 +332,34 @@ template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st)
 template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st) {
   return dispatch_len(a.g.Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
-    constexpr int W = tile_w<T>(NN);
-    const size_t smem = sizeof(V2<T>) * 4 * NN * W;
-    dim3 grid(a.g.Mzp / W, a.g.My);
-    k_p3<T, NN, W><<<grid, NT, smem, st>>>(a);
+    constexpr int W = tile_wp<T>(NN);
+    const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
+    const size_t smem = p_smem<T, NN>(W, a.g.Mx);
+    static int cache = 0;
+    k_p3<T, NN, W><<<resident_grid(k_p3<T, NN, W>, NTP, p_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
+        a, nzt, ntiles);
     return cudaGetLastError();
   });
+}
+
+template <typename K> cudaError_t max_smem(K kernel, int bytes) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
 }
 
 template <typename T> cudaError_t prepare_axis_kernels(int Nx) {
   return dispatch_len(Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
-    constexpr int W = tile_w<T>(NN);
-    const int smem = (int)(sizeof(V2<T>) * 4 * NN * W);
-    cudaError_t e = cudaFuncSetAttribute(k_p1<T, NN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    constexpr int WP = tile_wp<T>(NN);
+    const int smem = (int)p_smem<T, NN>(WP, NN);  // upper bound (Mx <= N)
+    cudaError_t e = max_smem(k_p1<T, NN, WP>, smem);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_p3<T, NN, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if ((e = max_smem(k_p3<T, NN, WP>, smem)) != cudaSuccess) return e;
+    constexpr int W = tile_w<T>(NN);
+    const int sa = (int)axis_smem<T, NN, W>();
+    if ((e = max_smem(k_axis<T, NN, W, true>, sa)) != cudaSuccess) return e;
+    return max_smem(k_axis<T, NN, W, false>, sa);
   });
 }
 
@@ -320,5 +373,7 @@ template cudaError_t prepare_axis_kernels<float>(int);
 template cudaError_t prepare_axis_kernels<double>(int);
 template int p3_tile_w<float>(int);
 template int p3_tile_w<double>(int);
+template int axis_tile_w<float>(int);
+template int axis_tile_w<double>(int);
 
 }  // namespace hit

@@ -9,10 +9,13 @@
 //   r2c: z[m] = x[2m] + i x[2m+1], Z = FFT_H(z),
 //        X[k] = (Z[k] + conj Z[H-k])/2 - i e^{-2 pi i k/Nz} (Z[k] - conj Z[H-k])/2.
 //
-// k_zcross fuses the middle of the RHS (src/hit3d/navierstokes.py:78-89): c2r of
-// u and w (6 rows), the pointwise u x w in physical space, r2c of the 3
-// products, all in shared memory, writing the products over the first three
-// input components of the same rows.
+// k_zcross fuses the middle of the RHS (src/hit3d/navierstokes.py:78-89): for RB
+// (x, y) rows, the c2r of u and w (6 rows each) runs as one batch whose last
+// stage leaves the physical values in shared memory; the forward transform's
+// first stage forms u x w from them; its last stage leaves the spectrum in
+// shared memory for the r2c post-processing, which writes the three products
+// over the first three input components of the same rows.
+#include <cstdlib>
 #include <type_traits>
 
 #include "fft_core.cuh"
@@ -20,11 +23,21 @@
 
 namespace hit {
 
-template <int H> constexpr int z_rows_per_block() { return (1024 / H) > 32 ? 32 : (1024 / H < 1 ? 1 : 1024 / H); }
+template <int H> __host__ __device__ constexpr int z_rows_per_block() {
+  return (1024 / H) > 32 ? 32 : (1024 / H < 1 ? 1 : 1024 / H);
+}
+// threads per block: one per last-stage butterfly of the 3*RB forward rows
+template <int H> __host__ __device__ constexpr int z_threads() {
+  return ((3 * z_rows_per_block<H>() * (H / fft16_radix(H, fft16_nstages(H) - 1)) + 31) / 32 * 32) < 96
+             ? 96
+             : ((3 * z_rows_per_block<H>() * (H / fft16_radix(H, fft16_nstages(H) - 1)) + 31) / 32 * 32);
+}
+// rows of Mzp entries are at most this long (Mzp <= round_up(H+1, 8))
+template <int H> __host__ __device__ constexpr int z_row_cap() { return (H + 1 + 7) / 8 * 8; }
 
 // conj-paired pre-processing of one c2r row element k in [0, H).
 template <typename T>
-__device__ __forceinline__ V2<T> c2r_pre(const V2<T>* row, int k, int H, int Mz, const V2<T>* tw, int twstep) {
+__device__ __forceinline__ V2<T> c2r_pre(const V2<T>* row, int k, int H, int Mz, const V2<T>* twz) {
   V2<T> X = k < Mz ? row[k] : czero<T>();
   const int kk = H - k;  // in [1, H]
   V2<T> Y = kk < Mz ? row[kk] : czero<T>();
@@ -34,126 +47,174 @@ __device__ __forceinline__ V2<T> c2r_pre(const V2<T>* row, int k, int H, int Mz,
   }
   Y.y = -Y.y;  // conj X[H-k]
   const V2<T> s = cadd(X, Y), d = csub(X, Y);
-  V2<T> w = __ldg(&tw[k * twstep]);
+  V2<T> w = twz[k];
   w.y = -w.y;  // e^{+2 pi i k / Nz}
   return cadd(s, cmul_i(cmul(w, d)));
 }
 
-// r2c post-processing: output bin k in [0, H] from Z (length H, row stride 1).
-template <typename T>
-__device__ __forceinline__ V2<T> r2c_post(const V2<T>* Z, int k, int H, const V2<T>* tw, int twstep) {
-  const V2<T> a = Z[k == H ? 0 : k];
-  V2<T> b = Z[k == 0 ? 0 : H - k];
+// r2c post-processing: output bin k in [0, H] from Z (length H), Z[i] = z(i).
+template <typename T, class ZF>
+__device__ __forceinline__ V2<T> r2c_post(ZF&& z, int k, int H, const V2<T>* twz) {
+  const V2<T> a = z(k == H ? 0 : k);
+  V2<T> b = z(k == 0 ? 0 : H - k);
   b.y = -b.y;
   const V2<T> E = cscale(cadd(a, b), T(0.5));
   const V2<T> O = cmul_mi(cscale(csub(a, b), T(0.5)));
-  const V2<T> w = __ldg(&tw[k * twstep]);  // e^{-2 pi i k / Nz}
+  const V2<T> w = twz[k];  // e^{-2 pi i k / Nz}
   return cadd(E, cmul(w, O));
 }
 
-template <typename T, int H, int RB>
-__global__ void __launch_bounds__(NT) k_zcross(ZCrossArgs<T> a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int LD = H + 1;
-  constexpr int twstep = TWN / (2 * H);
-  V2<T>* Z = reinterpret_cast<V2<T>*>(smem_raw);  // [6*RB][LD]
-  const long long row0 = (long long)blockIdx.x * RB;
-
-  for (int e = threadIdx.x; e < 6 * RB * H; e += NT) {
-    const int q = e / (RB * H), rem = e % (RB * H), lr = rem / H, k = rem % H;
-    const long long row = row0 + lr;
-    V2<T> v = czero<T>();
-    if (row < a.nrows) v = c2r_pre<T>(a.buf + q * a.c_stride + row * a.Mzp, k, H, a.Mz, a.tw, twstep);
-    Z[(q * RB + lr) * LD + k] = v;
-  }
+// Shared twiddles of the z kernels: the FFT stage tables (length H, radix-16
+// plan) followed by exp(-2 pi i k / Nz) for k in [0, H].
+template <int H> __host__ __device__ constexpr int z_tw_slots() { return (tw_size<true>(H) + H + 1 + 1) / 2 * 2; }
+// (an even slot count keeps whatever follows the tables 16-byte aligned)
+template <typename T, int H, int NTH>
+__device__ __forceinline__ void fill_z_twiddles(V2<T>* tws, const V2<T>* __restrict__ tw) {
+  fill_stage_twiddles<T, H, true, NTH>(tws, tw);
+  V2<T>* twz = tws + tw_size<true>(H);
+  for (int k = threadIdx.x; k <= H; k += NTH) twz[k] = tw[k * (TWN / (2 * H))];
   __syncthreads();
-  smem_fft<T, H, 6 * RB, NT, 1, LD, true>(Z, a.tw);
-
-  // u x w in physical space (navierstokes.py:82-86), on both halves of each pair
-  for (int e = threadIdx.x; e < RB * H; e += NT) {
-    const int lr = e / H, m = e % H;
-    V2<T> u[3], w[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      u[c] = cscale(Z[(c * RB + lr) * LD + m], a.scale);
-      w[c] = cscale(Z[((3 + c) * RB + lr) * LD + m], a.scale);
-    }
-    V2<T> n0, n1, n2;
-    n0.x = u[1].x * w[2].x - u[2].x * w[1].x;
-    n0.y = u[1].y * w[2].y - u[2].y * w[1].y;
-    n1.x = u[2].x * w[0].x - u[0].x * w[2].x;
-    n1.y = u[2].y * w[0].y - u[0].y * w[2].y;
-    n2.x = u[0].x * w[1].x - u[1].x * w[0].x;
-    n2.y = u[0].y * w[1].y - u[1].y * w[0].y;
-    Z[(0 * RB + lr) * LD + m] = n0;
-    Z[(1 * RB + lr) * LD + m] = n1;
-    Z[(2 * RB + lr) * LD + m] = n2;
-  }
-  __syncthreads();
-  smem_fft<T, H, 3 * RB, NT, 1, LD, false>(Z, a.tw);
-
-  for (int e = threadIdx.x; e < 3 * RB * a.Mzp; e += NT) {
-    const int q = e / (RB * a.Mzp), rem = e % (RB * a.Mzp), lr = rem / a.Mzp, k = rem % a.Mzp;
-    const long long row = row0 + lr;
-    if (row < a.nrows) {
-      V2<T> v = czero<T>();
-      if (k < a.Mz) v = r2c_post<T>(Z + (q * RB + lr) * LD, k, H, a.tw, twstep);
-      a.buf[q * a.c_stride + row * a.Mzp + k] = v;
-    }
-  }
 }
 
-template <typename T, int H, int RB>
-__global__ void __launch_bounds__(NT) k_zc2r(ZRealArgs<T> a) {
+template <typename T, int H, int RB, int NTZ, int MINB>
+__global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int LD = H + 1;
-  constexpr int twstep = TWN / (2 * H);
-  V2<T>* Z = reinterpret_cast<V2<T>*>(smem_raw);
-  const long long row0 = (long long)blockIdx.x * RB;
-  const long long c = blockIdx.y;
-  for (int e = threadIdx.x; e < RB * H; e += NT) {
-    const int lr = e / H, k = e % H;
-    const long long row = row0 + lr;
-    V2<T> v = czero<T>();
-    if (row < a.nrows) v = c2r_pre<T>(a.cbuf + c * a.cc_stride + row * a.Mzp, k, H, a.Mz, a.tw, twstep);
-    Z[lr * LD + k] = v;
-  }
-  __syncthreads();
-  smem_fft<T, H, RB, NT, 1, LD, true>(Z, a.tw);
-  for (int e = threadIdx.x; e < RB * H; e += NT) {
-    const int lr = e / H, m = e % H;
-    const long long row = row0 + lr;
-    if (row < a.nrows) {
-      V2<T>* out = reinterpret_cast<V2<T>*>(a.rbuf + c * a.rc_stride + row * (2 * H));
-      out[m] = cscale(Z[lr * LD + m], a.scale);
+  using AD = SkewAddr<skew_ld(H)>;
+  constexpr int KC = z_row_cap<H>();  // >= Mzp: slots per staged row
+  V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);  // 6*RB columns of AD::LD slots
+  V2<T>* tws = buf + 6 * RB * AD::LD;
+  const V2<T>* twz = tws + tw_size<true>(H);
+  V2<T>* raw = tws + z_tw_slots<H>();  // next group's input rows: [q*RB + lr][KC]
+  fill_z_twiddles<T, H, NTZ>(tws, a.tw);
+  const int ngroups = (a.nrows + RB - 1) / RB;
+  const int Mz = a.Mz, Mzp = a.Mzp;
+  constexpr int VPC = 16 / sizeof(V2<T>);  // complex values per 16-byte copy
+
+  // stage the 6 component rows of a group (rows past the end are zero-filled)
+  auto prefetch = [&](int grp) {
+    const long long r0 = (long long)grp * RB;
+    const int chunks = Mzp / VPC;  // Mzp is a multiple of 8: whole 16-byte chunks
+    for (int e = threadIdx.x; e < 6 * RB * chunks; e += NTZ) {
+      const int col = e / chunks, ch = e % chunks;
+      const int q = col / RB, lr = col % RB;
+      V2<T>* dst = raw + col * KC + ch * VPC;
+      if (r0 + lr < a.nrows) cp_async16(dst, a.buf + q * a.c_stride + (r0 + lr) * Mzp + ch * VPC);
+      else
+        for (int i = 0; i < VPC; ++i) dst[i] = czero<T>();
     }
+    cp_async_commit();
+  };
+
+  int grp = blockIdx.x;
+  if (grp < ngroups) prefetch(grp);
+  for (; grp < ngroups; grp += gridDim.x) {
+    const long long row0 = (long long)grp * RB;
+    const bool full = row0 + RB <= a.nrows;
+    cp_async_wait_all();
+    __syncthreads();
+
+    // c2r of the 6 components of RB rows (column = q*RB + lr) from the staged
+    // rows; as soon as every thread holds its first-stage inputs the staging
+    // buffer is refilled with the next group while this one is transformed
+    const int nxt = grp + gridDim.x;
+    fft_ip<T, H, 6 * RB, NTZ, AD, true>(
+        buf, tws,
+        [&](int k, int col) {
+          const V2<T>* row = raw + col * KC;
+          V2<T> X = k < Mz ? row[k] : czero<T>();
+          const int kk = H - k;
+          V2<T> Y = kk < Mz ? row[kk] : czero<T>();
+          if (k == 0) {
+            X.y = T(0);
+            Y.y = T(0);
+          }
+          Y.y = -Y.y;
+          const V2<T> sm = cadd(X, Y), df = csub(X, Y);
+          V2<T> w = twz[k];
+          w.y = -w.y;
+          return cadd(sm, cmul_i(cmul(w, df)));
+        },
+        [&](int m, int col, V2<T> v) { buf[AD::at(m, col)] = v; },
+        [&]() {
+          if (nxt < ngroups) prefetch(nxt);
+        });
+
+    // r2c of u x w (navierstokes.py:82-86), formed while loading the first stage
+    const T s2 = a.scale * a.scale;
+    fft_ip<T, H, 3 * RB, NTZ, AD, false>(
+        buf, tws,
+        [&](int m, int col) {
+          const int c = col / RB, lr = col % RB;
+          const int c1 = c == 2 ? 0 : c + 1, c2 = c == 0 ? 2 : c - 1;  // (1,2), (2,0), (0,1)
+          const V2<T> ua = buf[AD::at(m, c1 * RB + lr)], ub = buf[AD::at(m, c2 * RB + lr)];
+          const V2<T> wa = buf[AD::at(m, (3 + c1) * RB + lr)], wb = buf[AD::at(m, (3 + c2) * RB + lr)];
+          V2<T> n;
+          n.x = (ua.x * wb.x - ub.x * wa.x) * s2;
+          n.y = (ua.y * wb.y - ub.y * wa.y) * s2;
+          return n;
+        },
+        [&](int k, int col, V2<T> v) { buf[AD::at(k, col)] = v; });
+
+    for (int e = threadIdx.x; e < 3 * RB * KC; e += NTZ) {
+      const int col = e / KC, k = e % KC;
+      const int q = col / RB, lr = col % RB;
+      if ((full || row0 + lr < a.nrows) && k < Mzp) {
+        V2<T> v = czero<T>();
+        if (k < Mz) v = r2c_post<T>([&](int i) { return buf[AD::at(i, col)]; }, k, H, twz);
+        a.buf[q * a.c_stride + (row0 + lr) * Mzp + k] = v;
+      }
+    }
+    __syncthreads();  // buf is rewritten by the next group
   }
+  cp_async_wait_all();
 }
 
-template <typename T, int H, int RB>
-__global__ void __launch_bounds__(NT) k_zr2c(ZRealArgs<T> a) {
+template <typename T, int H, int RB, int NTZ>
+__global__ void __launch_bounds__(NTZ) k_zc2r(ZRealArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int LD = H + 1;
-  constexpr int twstep = TWN / (2 * H);
-  V2<T>* Z = reinterpret_cast<V2<T>*>(smem_raw);
+  using AD = SkewAddr<skew_ld(H)>;
+  V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* tws = buf + RB * AD::LD;
+  const V2<T>* twz = tws + tw_size<true>(H);
+  fill_z_twiddles<T, H, NTZ>(tws, a.tw);
   const long long row0 = (long long)blockIdx.x * RB;
   const long long c = blockIdx.y;
-  for (int e = threadIdx.x; e < RB * H; e += NT) {
-    const int lr = e / H, m = e % H;
-    const long long row = row0 + lr;
-    V2<T> v = czero<T>();
-    if (row < a.nrows) v = reinterpret_cast<const V2<T>*>(a.rbuf + c * a.rc_stride + row * (2 * H))[m];
-    Z[lr * LD + m] = v;
-  }
-  __syncthreads();
-  smem_fft<T, H, RB, NT, 1, LD, false>(Z, a.tw);
-  for (int e = threadIdx.x; e < RB * a.Mzp; e += NT) {
-    const int lr = e / a.Mzp, k = e % a.Mzp;
-    const long long row = row0 + lr;
-    if (row < a.nrows) {
+  fft_ip<T, H, RB, NTZ, AD, true>(
+      buf, tws,
+      [&](int k, int lr) {
+        if (row0 + lr >= a.nrows) return czero<T>();
+        return c2r_pre<T>(a.cbuf + c * a.cc_stride + (row0 + lr) * a.Mzp, k, H, a.Mz, twz);
+      },
+      [&](int m, int lr, V2<T> v) {
+        if (row0 + lr < a.nrows)
+          reinterpret_cast<V2<T>*>(a.rbuf + c * a.rc_stride + (row0 + lr) * (2 * H))[m] = cscale(v, a.scale);
+      });
+}
+
+template <typename T, int H, int RB, int NTZ>
+__global__ void __launch_bounds__(NTZ) k_zr2c(ZRealArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  using AD = SkewAddr<skew_ld(H)>;
+  constexpr int KC = z_row_cap<H>();
+  V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* tws = buf + RB * AD::LD;
+  const V2<T>* twz = tws + tw_size<true>(H);
+  fill_z_twiddles<T, H, NTZ>(tws, a.tw);
+  const long long row0 = (long long)blockIdx.x * RB;
+  const long long c = blockIdx.y;
+  fft_ip<T, H, RB, NTZ, AD, false>(
+      buf, tws,
+      [&](int m, int lr) {
+        if (row0 + lr >= a.nrows) return czero<T>();
+        return reinterpret_cast<const V2<T>*>(a.rbuf + c * a.rc_stride + (row0 + lr) * (2 * H))[m];
+      },
+      [&](int k, int lr, V2<T> v) { buf[AD::at(k, lr)] = v; });
+  for (int e = threadIdx.x; e < RB * KC; e += NTZ) {
+    const int lr = e / KC, k = e % KC;
+    if (row0 + lr < a.nrows && k < a.Mzp) {
       V2<T> v = czero<T>();
-      if (k < a.Mz) v = r2c_post<T>(Z + lr * LD, k, H, a.tw, twstep);
-      a.cbuf[c * a.cc_stride + row * a.Mzp + k] = v;
+      if (k < a.Mz) v = r2c_post<T>([&](int i) { return buf[AD::at(i, lr)]; }, k, H, twz);
+      a.cbuf[c * a.cc_stride + (row0 + lr) * a.Mzp + k] = v;
     }
   }
 }
@@ -173,14 +234,42 @@ template <typename F> cudaError_t dispatch_half(int H, F&& f) {
   }
 }
 
+template <typename T, int H> constexpr size_t zreal_smem() {
+  return sizeof(V2<T>) * (z_rows_per_block<H>() * skew_ld(H) + z_tw_slots<H>());
+}
+
+template <typename T, int HH, int RB, int NTZ, int MINB> cudaError_t launch_zcross_v(const ZCrossArgs<T>& a, cudaStream_t st) {
+  static bool ready = false;
+  const size_t smem = sizeof(V2<T>) * (6 * RB * skew_ld(HH) + z_tw_slots<HH>() + 6 * RB * z_row_cap<HH>());
+  static int cache = 0;
+  if (!ready) {
+    cudaError_t e = cudaFuncSetAttribute(k_zcross<T, HH, RB, NTZ, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_zcross<T, HH, RB, NTZ, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    ready = true;
+  }
+  const int nb = resident_grid(k_zcross<T, HH, RB, NTZ, MINB>, NTZ, smem, (a.nrows + RB - 1) / RB, cache);
+  k_zcross<T, HH, RB, NTZ, MINB><<<nb, NTZ, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, cudaStream_t st) {
+  static int cfg = [] { const char* e = getenv("HIT_ZCFG"); return e ? atoi(e) : 0; }();
+  if (H == 256) {
+    switch (cfg) {
+      case 1: return launch_zcross_v<T, 256, 1, 32, 1>(a, st);
+      case 2: return launch_zcross_v<T, 256, 2, 64, 1>(a, st);
+      case 3: return launch_zcross_v<T, 256, 4, 384, 1>(a, st);
+      case 4: return launch_zcross_v<T, 256, 2, 96, 1>(a, st);
+      default: break;
+    }
+  }
   return dispatch_half(H, [&](auto hh) {
     constexpr int HH = decltype(hh)::value;
     constexpr int RB = z_rows_per_block<HH>();
-    const size_t smem = sizeof(V2<T>) * 6 * RB * (HH + 1);
-    const int nb = (a.nrows + RB - 1) / RB;
-    k_zcross<T, HH, RB><<<nb, NT, smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_zcross_v<T, HH, RB, z_threads<HH>(), 2>(a, st);
   });
 }
 
@@ -188,9 +277,8 @@ template <typename T> cudaError_t launch_zc2r(int H, const ZRealArgs<T>& a, int 
   return dispatch_half(H, [&](auto hh) {
     constexpr int HH = decltype(hh)::value;
     constexpr int RB = z_rows_per_block<HH>();
-    const size_t smem = sizeof(V2<T>) * RB * (HH + 1);
     dim3 grid((a.nrows + RB - 1) / RB, ncomp);
-    k_zc2r<T, HH, RB><<<grid, NT, smem, st>>>(a);
+    k_zc2r<T, HH, RB, z_threads<HH>()><<<grid, z_threads<HH>(), zreal_smem<T, HH>(), st>>>(a);
     return cudaGetLastError();
   });
 }
@@ -199,24 +287,31 @@ template <typename T> cudaError_t launch_zr2c(int H, const ZRealArgs<T>& a, int 
   return dispatch_half(H, [&](auto hh) {
     constexpr int HH = decltype(hh)::value;
     constexpr int RB = z_rows_per_block<HH>();
-    const size_t smem = sizeof(V2<T>) * RB * (HH + 1);
     dim3 grid((a.nrows + RB - 1) / RB, ncomp);
-    k_zr2c<T, HH, RB><<<grid, NT, smem, st>>>(a);
+    k_zr2c<T, HH, RB, z_threads<HH>()><<<grid, z_threads<HH>(), zreal_smem<T, HH>(), st>>>(a);
     return cudaGetLastError();
   });
 }
 
 template <typename T> cudaError_t prepare_axis_kernels(int Nx);
 
+template <typename K> cudaError_t max_smem(K kernel, int bytes) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+}
+
 template <typename T> cudaError_t prepare_fft_kernels(int Nx, int Ny, int Nz) {
-  (void)Ny;
   cudaError_t e = prepare_axis_kernels<T>(Nx);
   if (e != cudaSuccess) return e;
+  if (Ny != Nx && (e = prepare_axis_kernels<T>(Ny)) != cudaSuccess) return e;
   return dispatch_half(Nz / 2, [&](auto hh) {
     constexpr int HH = decltype(hh)::value;
     constexpr int RB = z_rows_per_block<HH>();
-    const int smem = (int)(sizeof(V2<T>) * 6 * RB * (HH + 1));
-    return cudaFuncSetAttribute(k_zcross<T, HH, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    constexpr int NTZ = z_threads<HH>();
+    cudaError_t r = max_smem(k_zc2r<T, HH, RB, NTZ>, (int)zreal_smem<T, HH>());
+    if (r != cudaSuccess) return r;
+    return max_smem(k_zr2c<T, HH, RB, NTZ>, (int)zreal_smem<T, HH>());
   });
 }
 

@@ -9,13 +9,16 @@
 
 namespace hit {
 
-constexpr int NT = 256;  // threads per block of every FFT kernel
+constexpr int NT = 256;   // threads per block of the axis, z and reduction kernels
+constexpr int NTP = 512;  // threads per block of k_p1/k_p3 (one 131 KB CTA per SM)
 
 // Columns (contiguous z entries) per x/y tile: one tile column block is at
 // most 32 KB, so P1/P3 (four tiles) fit in 128 KB of shared memory.
-template <typename T> constexpr int tile_w(int N) {
+template <typename T> __host__ __device__ constexpr int tile_w(int N) {
   return (32768 / (N * (int)sizeof(V2<T>))) >= 8 ? 8 : (32768 / (N * (int)sizeof(V2<T>)));
 }
+// k_p1/k_p3 tile width (same as the axis kernels).
+template <typename T> __host__ __device__ constexpr int tile_wp(int N) { return tile_w<T>(N); }
 
 // Plain column FFT along a strided axis ("a") of a 4-D array indexed
 // (comp, a, o, z): element at src + c*s_c + a*s_a + o*s_o + z.  Input rows
@@ -88,6 +91,19 @@ template <typename T> struct ZRealArgs {
   const V2<T>* tw;
 };
 
+// Persistent launch size: the number of blocks that stay resident (the FFT
+// kernels loop over their tiles, filling their shared twiddle tables once).
+template <typename K> int resident_grid(K kernel, int threads, size_t smem, long long ntiles, int& cache) {
+  if (cache == 0) {
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem);
+    cache = (occ > 0 ? occ : 1) * (sms > 0 ? sms : 1);
+  }
+  return (int)(ntiles < cache ? (ntiles > 0 ? ntiles : 1) : cache);
+}
+
 // Launchers (return cudaError_t of the launch).
 template <typename T> cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, int nc, cudaStream_t st);
 template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st);
@@ -99,6 +115,7 @@ template <typename T> cudaError_t prepare_fft_kernels(int Nx, int Ny, int Nz);
 template <typename T> cudaError_t prepare_axis_kernels(int Nx);
 int p3_num_blocks(const Geom& g, int W);
 template <typename T> int p3_tile_w(int Nx);
+template <typename T> int axis_tile_w(int N);
 
 // ---- reductions / elementwise (k_reduce.cu) ----------------------------------
 // Scalar sums over modes: index 0: sum w|u|^2, 1: sum w k2 |u|^2, 2: band sum w|u|^2

@@ -294,7 +294,7 @@ template <typename T> int launch_p1_of(hit_plan* p, Path& P, const V2<T>* src, c
 template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st, Prof* pf = nullptr) {
   const Geom& g = P.g;
   const long long t6c = (long long)g.Nx * g.My * g.Mzp, u6c = (long long)g.Nx * g.Ny * g.Mzp;
-  const int Wy = p3_tile_w<T>(g.Ny);
+  const int Wy = axis_tile_w<T>(g.Ny);
   AxisArgs<T> a{};
   a.src = vp<T>(P.t6);
   a.dst = vp<T>(P.u6);
@@ -480,7 +480,7 @@ template <typename T> int to_physical_impl(hit_plan* p, const void* u_hat, int n
   const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
   int rc;
   if ((rc = ensure(p->xws, (size_t)nc * g.Nx * g.Ny * g.Mzp * sizeof(V2<T>)))) return rc;
-  const int Wx = p3_tile_w<T>(g.Nx), Wy = p3_tile_w<T>(g.Ny);
+  const int Wx = axis_tile_w<T>(g.Nx), Wy = axis_tile_w<T>(g.Ny);
   const long long wc = (long long)g.Nx * g.Ny * g.Mzp;
   AxisArgs<T> a{};
   a.src = static_cast<const V2<T>*>(u_hat);
@@ -525,7 +525,7 @@ template <typename T> int to_spectral_impl(hit_plan* p, const void* u, int nc, v
   const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
   int rc;
   if ((rc = ensure(p->xws, (size_t)nc * g.Nx * g.Ny * g.Mzp * sizeof(V2<T>)))) return rc;
-  const int Wx = p3_tile_w<T>(g.Nx), Wy = p3_tile_w<T>(g.Ny);
+  const int Wx = axis_tile_w<T>(g.Nx), Wy = axis_tile_w<T>(g.Ny);
   const long long wc = (long long)g.Nx * g.Ny * g.Mzp;
   ZRealArgs<T> z{};
   z.cbuf = vp<T>(p->xws);
