@@ -16,6 +16,8 @@
 // rows (z pass).
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace hit {
@@ -174,6 +176,10 @@ template <bool INV, typename V> struct DFT<16, INV, V> {
   }
 };
 
+struct NoHook {
+  __device__ void operator()() const {}
+};
+
 // One Stockham stage.  SRC/DST: 0 = functor, 1 = buffer A, 2 = buffer B.
 template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, int R, int P, int TWO, int SRC, int DST,
           class LD, class ST>
@@ -216,15 +222,19 @@ __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __res
   if (DST != 0) __syncthreads();
 }
 
-template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, int S, class LD, class ST>
-__device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* tws, LD& ld, ST& st) {
+template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, int S, class LD, class ST, class HK>
+__device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* tws, LD& ld, ST& st, HK& hk) {
   constexpr int NS = fft_nstages(N);
   if constexpr (S < NS) {
     constexpr int SRC = S == 0 ? 0 : ((S - 1) % 2 == 0 ? 1 : 2);
     constexpr int DST = S == NS - 1 ? 0 : (S % 2 == 0 ? 1 : 2);
     fft_stage_io<T, N, NCOLS, NT, SP, SC, INV, fft_radix(N, S), fft_pprod(N, S), tw_offset<false>(N, S), SRC, DST>(
         A, B, tws, ld, st);
-    fft_stages_io<T, N, NCOLS, NT, SP, SC, INV, S + 1>(A, B, tws, ld, st);
+    if constexpr (S == 0 && !std::is_same<HK, NoHook>::value) {
+      if constexpr (DST == 0) __syncthreads();
+      hk();
+    }
+    fft_stages_io<T, N, NCOLS, NT, SP, SC, INV, S + 1>(A, B, tws, ld, st, hk);
   }
 }
 
@@ -236,10 +246,13 @@ __device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* t
 // after st writes shared memory that other threads read.  The storer may write
 // into buffer fft_free_buffer(N) (0 = A, 1 = B), which the last stage does not
 // read.
-template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, class LD, class ST>
-__device__ __forceinline__ void fft_io(V2<T>* A, V2<T>* B, const V2<T>* tws, LD&& ld, ST&& st) {
+// after_stage0() (optional) runs once every thread has finished the first
+// stage, when the loader's source may be reused.
+template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, class LD, class ST, class HK = NoHook>
+__device__ __forceinline__ void fft_io(V2<T>* A, V2<T>* B, const V2<T>* tws, LD&& ld, ST&& st,
+                                       HK&& after_stage0 = HK{}) {
   static_assert((N & (N - 1)) == 0 && N >= 2 && N <= TWN, "power-of-two length");
-  fft_stages_io<T, N, NCOLS, NT, SP, SC, INV, 0>(A, B, tws, ld, st);
+  fft_stages_io<T, N, NCOLS, NT, SP, SC, INV, 0>(A, B, tws, ld, st, after_stage0);
 }
 
 // ---------------------------------------------------------------------------
@@ -322,10 +335,6 @@ __device__ __forceinline__ void fft_ip_stages(V2<T>* buf, const V2<T>* tws, LD& 
 // last stage calls st(pos, col, v) (which may write buf).  Radix-16 plan,
 // twiddles from the shared stage tables tws (fill_stage_twiddles<T, N, true>).
 // Returns with the block synchronised.
-struct NoHook {
-  __device__ void operator()() const {}
-};
-
 // after_loads() runs once, right after every thread has loaded the inputs of
 // the first stage (the loader's source is then free for reuse).
 template <typename T, int N, int NCOLS, int NT, class ADDR, bool INV, class LD, class ST, class HK = NoHook>

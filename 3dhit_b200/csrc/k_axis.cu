@@ -15,6 +15,7 @@
 //         projection (grid.py:166-178), viscous term (navierstokes.py:95) and
 //         the RK4 stage algebra (integrators.py:32-38), then -- fused -- the
 //         next stage's k_p1 on the tile it just produced.
+#include <cstdint>
 #include <type_traits>
 
 #include "fft_core.cuh"
@@ -22,13 +23,32 @@
 
 namespace hit {
 
-template <typename T, int N, int W, bool INV>
+// PF: the next tile's stored rows are staged in shared memory with cp.async
+// while the current tile is transformed (needs 16-byte aligned rows/columns).
+template <typename T, int N, int W, bool INV, bool PF>
 __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
   V2<T>* B = A + N * W;
   V2<T>* tws = B + N * W;
+  V2<T>* stg = tws + ((tw_size<false>(N) + 1) / 2 * 2);  // PF: Min x W staged rows
   fill_stage_twiddles<T, N, false, NT>(tws, a.tw);
+  constexpr int VPC = 16 / sizeof(V2<T>);
+  auto tile_src = [&](int tile) {
+    const int zt = tile % nzt, rest = tile / nzt;
+    const long long o = rest % no, c = rest / no;
+    return a.src + c * a.s_c + o * a.s_o + zt * W;
+  };
+  auto prefetch = [&](int tile) {
+    const V2<T>* src = tile_src(tile);
+    constexpr int CPR = W / VPC;  // 16-byte chunks per row
+    for (int e = threadIdx.x; e < a.Min * CPR; e += NT) {
+      const int row = e / CPR, ch = e % CPR;
+      cp_async16(stg + row * W + ch * VPC, src + (long long)row * a.s_a + ch * VPC);
+    }
+    cp_async_commit();
+  };
+  if (PF && blockIdx.x < ntiles) prefetch(blockIdx.x);
   __syncthreads();
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int zt = tile % nzt, rest = tile / nzt;
@@ -37,18 +57,28 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
     const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
     V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
     const bool zc = z0 + W <= a.nz;  // whole tile inside the valid columns
+    if (PF) {
+      cp_async_wait_all();
+      __syncthreads();
+    }
+    const int nxt = tile + gridDim.x;
     fft_io<T, N, W, NT, W, 1, INV>(
         A, B, tws,
         [&](int pos, int col) {
           const int row = compact_row(pos, a.hin, a.Min, N);
+          if (PF) return row >= 0 ? stg[row * W + col] : czero<T>();
           return (row >= 0 && (zc || z0 + col < a.nz)) ? src[(long long)row * a.s_a + col] : czero<T>();
         },
         [&](int pos, int col, V2<T> v) {
           const int row = compact_row(pos, a.hout, a.Mout, N);
           if (row >= 0 && (zc || z0 + col < a.nz)) dst[(long long)row * a.d_a + col] = v;
+        },
+        [&]() {
+          if (PF && nxt < ntiles) prefetch(nxt);
         });
     __syncthreads();  // the next tile's first stage rewrites A
   }
+  if (PF) cp_async_wait_all();
 }
 
 // x-inverse of u and w = i k x u for one (ky row, z tile).  S holds the three
@@ -99,7 +129,7 @@ __global__ void __launch_bounds__(NTP) k_p1(P1Args<T> a, int nzt, int ntiles) {
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
   V2<T>* B = A + N * W;
   V2<T>* tws = B + N * W;
-  V2<T>* S = tws + tw_size<false>(N);  // 3 x Mx x W
+  V2<T>* S = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W
   fill_stage_twiddles<T, N, false, NTP>(tws, a.tw);
   const int MW = g.Mx * W;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -116,18 +146,37 @@ __global__ void __launch_bounds__(NTP) k_p1(P1Args<T> a, int nzt, int ntiles) {
 
 template <typename T, int N, int W>
 __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, const V2<T>* tws, V2<T>* F, double* red,
-                                        int j, int z0, int tile) {
+                                        int j, int z0, int tile, V2<T>* stg, int nzt, int ntiles) {
   const Geom& g = a.g;
   const int MW = g.Mx * W;
+  constexpr int VPC = 16 / sizeof(V2<T>);
+  // staged x column of one nl component (N x W)
+  auto prefetch = [&](int t, int c, V2<T>* dstb) {
+    const int jj = t / nzt, zz = (t % nzt) * W;
+    const V2<T>* src = a.t3 + c * a.t_c + (long long)jj * g.Mzp + zz;
+    constexpr int CPR = W / VPC;
+    for (int e = threadIdx.x; e < N * CPR; e += NTP) {
+      const int row = e / CPR, ch = e % CPR;
+      cp_async16(dstb + row * W + ch * VPC, src + (long long)row * a.t_x + ch * VPC);
+    }
+    cp_async_commit();
+  };
 
-  const V2<T>* src = a.t3 + (long long)j * g.Mzp + z0;
 #pragma unroll 1
   for (int c = 0; c < 3; ++c) {
+    cp_async_wait_all();
+    __syncthreads();
+    // once the first stage has read the staged column, stage the next one:
+    // component c+1 of this tile, or component 0 of the next tile
     fft_io<T, N, W, NTP, W, 1, false>(
-        A, B, tws, [&](int pos, int col) { return src[c * a.t_c + (long long)pos * a.t_x + col]; },
+        A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; },
         [&](int pos, int col, V2<T> v) {
           const int row = compact_row(pos, g.hx, g.Mx, N);
           if (row >= 0) F[c * MW + row * W + col] = v;
+        },
+        [&]() {
+          if (c < 2) prefetch(tile, c + 1, stg);
+          else if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, 0, stg);
         });
     __syncthreads();
   }
@@ -249,14 +298,25 @@ __global__ void __launch_bounds__(NTP) k_p3(P3Args<T> a, int nzt, int ntiles) {
   __shared__ double red[32];
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
   V2<T>* B = A + N * W;
-  V2<T>* tws = B + N * W;
-  V2<T>* F = tws + tw_size<false>(N);  // 3 x Mx x W: nl, then the new stage input
+  V2<T>* stg = B + N * W;  // staged N x W column of the next nl component
+  V2<T>* tws = stg + N * W;
+  V2<T>* F = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W: nl, then the new stage input
   fill_stage_twiddles<T, N, false, NTP>(tws, a.tw);
-  __syncthreads();
+  if (blockIdx.x < ntiles) {
+    const int jj = blockIdx.x / nzt, zz = (blockIdx.x % nzt) * W;
+    const V2<T>* src = a.t3 + (long long)jj * a.g.Mzp + zz;
+    constexpr int VPC = 16 / sizeof(V2<T>), CPR = W / VPC;
+    for (int e = threadIdx.x; e < N * CPR; e += NTP) {
+      const int row = e / CPR, ch = e % CPR;
+      cp_async16(stg + row * W + ch * VPC, src + (long long)row * a.t_x + ch * VPC);
+    }
+    cp_async_commit();
+  }
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int j = tile / nzt, z0 = (tile % nzt) * W;
-    p3_tile<T, N, W>(a, A, B, tws, F, red, j, z0, tile);
+    p3_tile<T, N, W>(a, A, B, tws, F, red, j, z0, tile, stg, nzt, ntiles);
   }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -279,25 +339,46 @@ template <typename F> cudaError_t dispatch_len(int N, F&& f) {
 }
 
 // P1/P3 shared memory: A, B (N x W each) and the 3 compact tiles (Mx x W).
-template <typename T, int N> size_t p_smem(int W, int Mx) {
-  return sizeof(V2<T>) * ((size_t)(2 * N + 3 * Mx) * W + tw_size<false>(N));
+// (twiddle slots rounded to an even count keep what follows 16-byte aligned)
+template <int N> constexpr int tw_slots_even() { return (tw_size<false>(N) + 1) / 2 * 2; }
+template <typename T, int N> size_t p1_smem(int W, int Mx) {
+  return sizeof(V2<T>) * ((size_t)(2 * N + 3 * Mx) * W + tw_slots_even<N>());
 }
-template <typename T, int N, int W> constexpr size_t axis_smem() { return sizeof(V2<T>) * (2 * N * W + tw_size<false>(N)); }
+template <typename T, int N> size_t p3_smem(int W, int Mx) {
+  return sizeof(V2<T>) * ((size_t)(3 * N + 3 * Mx) * W + tw_slots_even<N>());
+}
+template <typename T, int N, int W, bool PF> constexpr size_t axis_smem() {
+  return sizeof(V2<T>) * ((PF ? 3 : 2) * N * W + tw_slots_even<N>());
+}
 
 template <typename T>
 cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, int nc, cudaStream_t st) {
   return dispatch_len(N, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
     constexpr int W = tile_w<T>(NN);
-    const size_t smem = axis_smem<T, NN, W>();
     const long long ntiles = (long long)nzt * no * nc;
-    static int c_inv = 0, c_fwd = 0;
-    if (inv)
-      k_axis<T, NN, W, true><<<resident_grid(k_axis<T, NN, W, true>, NT, smem, ntiles, c_inv), NT, smem, st>>>(
-          a, nzt, no, (int)ntiles);
-    else
-      k_axis<T, NN, W, false><<<resident_grid(k_axis<T, NN, W, false>, NT, smem, ntiles, c_fwd), NT, smem, st>>>(
-          a, nzt, no, (int)ntiles);
+    // staging needs 16-byte aligned rows and whole tiles
+    const bool pf = (sizeof(V2<T>) == 16 || ((a.s_a | a.s_o | a.s_c) % 2 == 0 &&
+                                              ((uintptr_t)a.src % 16) == 0)) &&
+                    a.nz % W == 0 && nzt * W == a.nz;
+    static int c[4] = {0, 0, 0, 0};
+    if (pf) {
+      const size_t smem = axis_smem<T, NN, W, true>();
+      if (inv)
+        k_axis<T, NN, W, true, true><<<resident_grid(k_axis<T, NN, W, true, true>, NT, smem, ntiles, c[0]), NT,
+                                       smem, st>>>(a, nzt, no, (int)ntiles);
+      else
+        k_axis<T, NN, W, false, true><<<resident_grid(k_axis<T, NN, W, false, true>, NT, smem, ntiles, c[1]), NT,
+                                        smem, st>>>(a, nzt, no, (int)ntiles);
+    } else {
+      const size_t smem = axis_smem<T, NN, W, false>();
+      if (inv)
+        k_axis<T, NN, W, true, false><<<resident_grid(k_axis<T, NN, W, true, false>, NT, smem, ntiles, c[2]), NT,
+                                        smem, st>>>(a, nzt, no, (int)ntiles);
+      else
+        k_axis<T, NN, W, false, false><<<resident_grid(k_axis<T, NN, W, false, false>, NT, smem, ntiles, c[3]),
+                                         NT, smem, st>>>(a, nzt, no, (int)ntiles);
+    }
     return cudaGetLastError();
   });
 }
@@ -321,9 +402,9 @@ template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st)
     constexpr int NN = decltype(nn)::value;
     constexpr int W = tile_wp<T>(NN);
     const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
-    const size_t smem = p_smem<T, NN>(W, a.g.Mx);
+    const size_t smem = p1_smem<T, NN>(W, a.g.Mx);
     static int cache = 0;
-    k_p1<T, NN, W><<<resident_grid(k_p1<T, NN, W>, NTP, p_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
+    k_p1<T, NN, W><<<resident_grid(k_p1<T, NN, W>, NTP, p1_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
         a, nzt, ntiles);
     return cudaGetLastError();
   });
@@ -334,9 +415,9 @@ template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st)
     constexpr int NN = decltype(nn)::value;
     constexpr int W = tile_wp<T>(NN);
     const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
-    const size_t smem = p_smem<T, NN>(W, a.g.Mx);
+    const size_t smem = p3_smem<T, NN>(W, a.g.Mx);
     static int cache = 0;
-    k_p3<T, NN, W><<<resident_grid(k_p3<T, NN, W>, NTP, p_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
+    k_p3<T, NN, W><<<resident_grid(k_p3<T, NN, W>, NTP, p3_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
         a, nzt, ntiles);
     return cudaGetLastError();
   });
@@ -352,14 +433,14 @@ template <typename T> cudaError_t prepare_axis_kernels(int Nx) {
   return dispatch_len(Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
     constexpr int WP = tile_wp<T>(NN);
-    const int smem = (int)p_smem<T, NN>(WP, NN);  // upper bound (Mx <= N)
-    cudaError_t e = max_smem(k_p1<T, NN, WP>, smem);
+    cudaError_t e = max_smem(k_p1<T, NN, WP>, (int)p1_smem<T, NN>(WP, NN));  // upper bounds (Mx <= N)
     if (e != cudaSuccess) return e;
-    if ((e = max_smem(k_p3<T, NN, WP>, smem)) != cudaSuccess) return e;
+    if ((e = max_smem(k_p3<T, NN, WP>, (int)p3_smem<T, NN>(WP, NN))) != cudaSuccess) return e;
     constexpr int W = tile_w<T>(NN);
-    const int sa = (int)axis_smem<T, NN, W>();
-    if ((e = max_smem(k_axis<T, NN, W, true>, sa)) != cudaSuccess) return e;
-    return max_smem(k_axis<T, NN, W, false>, sa);
+    if ((e = max_smem(k_axis<T, NN, W, true, true>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
+    if ((e = max_smem(k_axis<T, NN, W, false, true>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
+    if ((e = max_smem(k_axis<T, NN, W, true, false>, (int)axis_smem<T, NN, W, false>())) != cudaSuccess) return e;
+    return max_smem(k_axis<T, NN, W, false, false>, (int)axis_smem<T, NN, W, false>());
   });
 }
 
