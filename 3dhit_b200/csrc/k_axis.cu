@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
 
 // x-inverse of u and w = i k x u for one (ky row, z tile).  S holds the three
 // stage-input columns in compact rows (Mx x W each); A/B are the FFT buffers.
-template <typename T, int N, int W>
+template <typename T, int N, int W, int NTH>
 __device__ __forceinline__ void p1_body(const V2<T>* S, V2<T>* A, V2<T>* B, int j, int z0, const Geom& g,
                                         const KTab<T>& kt, const V2<T>* tws, V2<T>* t6, long long t_c,
                                         long long t_x) {
@@ -93,7 +93,7 @@ __device__ __forceinline__ void p1_body(const V2<T>* S, V2<T>* A, V2<T>* B, int 
   const int MW = g.Mx * W;
 #pragma unroll 1
   for (int q = 0; q < 6; ++q) {
-    fft_io<T, N, W, NTP, W, 1, true>(
+    fft_io<T, N, W, NTH, W, 1, true>(
         A, B, tws,
         [&](int pos, int col) {
           const int row = compact_row(pos, g.hx, g.Mx, N);
@@ -122,29 +122,35 @@ __device__ __forceinline__ void p1_body(const V2<T>* S, V2<T>* A, V2<T>* B, int 
   }
 }
 
-template <typename T, int N, int W>
-__global__ void __launch_bounds__(NTP) k_p1(P1Args<T> a, int nzt, int ntiles) {
+template <typename T, int N, int W, int NTH>
+__global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geom& g = a.g;
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
   V2<T>* B = A + N * W;
   V2<T>* tws = B + N * W;
   V2<T>* S = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W
-  fill_stage_twiddles<T, N, false, NTP>(tws, a.tw);
+  fill_stage_twiddles<T, N, false, NTH>(tws, a.tw);
   const int MW = g.Mx * W;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int j = tile / nzt, z0 = (tile % nzt) * W;
     const V2<T>* src = a.s + (long long)j * g.Mzp + z0;
-    for (int e = threadIdx.x; e < 3 * MW; e += NTP) {
+    const int nxt = tile + gridDim.x;
+    if (nxt < ntiles) {  // next tile's rows into L2 while this one is transformed
+      const V2<T>* ns = a.s + (long long)(nxt / nzt) * g.Mzp + (nxt % nzt) * W;
+      for (int e = threadIdx.x; e < 3 * g.Mx; e += NTH)
+        prefetch_l2(ns + (e / g.Mx) * a.s_c + (long long)(e % g.Mx) * a.s_x, W * sizeof(V2<T>));
+    }
+    for (int e = threadIdx.x; e < 3 * MW; e += NTH) {
       const int c = e / MW, r = e - c * MW;
       S[e] = src[c * a.s_c + (long long)(r / W) * a.s_x + r % W];
     }
     __syncthreads();
-    p1_body<T, N, W>(S, A, B, j, z0, g, a.k, tws, a.t6, a.t_c, a.t_x);
+    p1_body<T, N, W, NTH>(S, A, B, j, z0, g, a.k, tws, a.t6, a.t_c, a.t_x);
   }
 }
 
-template <typename T, int N, int W>
+template <typename T, int N, int W, int NTH>
 __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, const V2<T>* tws, V2<T>* F, double* red,
                                         int j, int z0, int tile, V2<T>* stg, int nzt, int ntiles) {
   const Geom& g = a.g;
@@ -155,12 +161,24 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     const int jj = t / nzt, zz = (t % nzt) * W;
     const V2<T>* src = a.t3 + c * a.t_c + (long long)jj * g.Mzp + zz;
     constexpr int CPR = W / VPC;
-    for (int e = threadIdx.x; e < N * CPR; e += NTP) {
+    for (int e = threadIdx.x; e < N * CPR; e += NTH) {
       const int row = e / CPR, ch = e % CPR;
       cp_async16(dstb + row * W + ch * VPC, src + (long long)row * a.t_x + ch * VPC);
     }
     cp_async_commit();
   };
+
+  // pull the state rows the epilogue reads into L2 while the forward
+  // transforms run (one 16-byte-aligned W-wide row segment per prefetch)
+  {
+    const int narr = a.stage <= 1 ? 1 : 3;  // u | s, acc, u
+    const V2<T>* arrs[3] = {a.stage <= 1 ? a.u : a.s, a.acc, a.u};
+    const long long cbase = (long long)j * g.Mzp + z0;
+    for (int e = threadIdx.x; e < narr * 3 * g.Mx; e += NTH) {
+      const int ar = e / (3 * g.Mx), rem = e % (3 * g.Mx), c = rem / g.Mx, i = rem % g.Mx;
+      prefetch_l2(arrs[ar] + c * a.c_c + (long long)i * a.c_x + cbase, W * sizeof(V2<T>));
+    }
+  }
 
 #pragma unroll 1
   for (int c = 0; c < 3; ++c) {
@@ -168,7 +186,7 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     __syncthreads();
     // once the first stage has read the staged column, stage the next one:
     // component c+1 of this tile, or component 0 of the next tile
-    fft_io<T, N, W, NTP, W, 1, false>(
+    fft_io<T, N, W, NTH, W, 1, false>(
         A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; },
         [&](int pos, int col, V2<T> v) {
           const int row = compact_row(pos, g.hx, g.Mx, N);
@@ -186,7 +204,7 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
   const T cf = (a.forcing == 2 || a.forcing == 3) ? T(a.coef[0]) : T(0);
   double sE = 0.0, sO = 0.0, sB = 0.0;
   const long long cbase = (long long)j * g.Mzp + z0;
-  for (int e = threadIdx.x; e < MW; e += NTP) {
+  for (int e = threadIdx.x; e < MW; e += NTH) {
     const int i = e / W, col = e % W, z = z0 + col;
     const int pos = full_pos(i, g.hx, g.Mx, N);
     V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
@@ -289,11 +307,11 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     if (threadIdx.x == 0) a.partial[3 * b + 2] = r;
   }
   __syncthreads();  // F complete; A/B free for the next tile or the fused x-inverse
-  if (a.fuse_p1) p1_body<T, N, W>(F, A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x);
+  if (a.fuse_p1) p1_body<T, N, W, NTH>(F, A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x);
 }
 
-template <typename T, int N, int W>
-__global__ void __launch_bounds__(NTP) k_p3(P3Args<T> a, int nzt, int ntiles) {
+template <typename T, int N, int W, int NTH>
+__global__ void __launch_bounds__(NTH) k_p3(P3Args<T> a, int nzt, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
@@ -301,12 +319,12 @@ __global__ void __launch_bounds__(NTP) k_p3(P3Args<T> a, int nzt, int ntiles) {
   V2<T>* stg = B + N * W;  // staged N x W column of the next nl component
   V2<T>* tws = stg + N * W;
   V2<T>* F = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W: nl, then the new stage input
-  fill_stage_twiddles<T, N, false, NTP>(tws, a.tw);
+  fill_stage_twiddles<T, N, false, NTH>(tws, a.tw);
   if (blockIdx.x < ntiles) {
     const int jj = blockIdx.x / nzt, zz = (blockIdx.x % nzt) * W;
     const V2<T>* src = a.t3 + (long long)jj * a.g.Mzp + zz;
     constexpr int VPC = 16 / sizeof(V2<T>), CPR = W / VPC;
-    for (int e = threadIdx.x; e < N * CPR; e += NTP) {
+    for (int e = threadIdx.x; e < N * CPR; e += NTH) {
       const int row = e / CPR, ch = e % CPR;
       cp_async16(stg + row * W + ch * VPC, src + (long long)row * a.t_x + ch * VPC);
     }
@@ -314,7 +332,7 @@ __global__ void __launch_bounds__(NTP) k_p3(P3Args<T> a, int nzt, int ntiles) {
   }
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int j = tile / nzt, z0 = (tile % nzt) * W;
-    p3_tile<T, N, W>(a, A, B, tws, F, red, j, z0, tile, stg, nzt, ntiles);
+    p3_tile<T, N, W, NTH>(a, A, B, tws, F, red, j, z0, tile, stg, nzt, ntiles);
   }
   cp_async_wait_all();
 }
@@ -397,45 +415,60 @@ template <typename T> int axis_tile_w(int N) {
 
 int p3_num_blocks(const Geom& g, int W) { return (g.Mzp / W) * g.My; }
 
-template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st) {
-  return dispatch_len(a.g.Nx, [&](auto nn) {
-    constexpr int NN = decltype(nn)::value;
-    constexpr int W = tile_wp<T>(NN);
-    const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
-    const size_t smem = p1_smem<T, NN>(W, a.g.Mx);
-    static int cache = 0;
-    k_p1<T, NN, W><<<resident_grid(k_p1<T, NN, W>, NTP, p1_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
-        a, nzt, ntiles);
-    return cudaGetLastError();
-  });
-}
-
-template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st) {
-  return dispatch_len(a.g.Nx, [&](auto nn) {
-    constexpr int NN = decltype(nn)::value;
-    constexpr int W = tile_wp<T>(NN);
-    const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
-    const size_t smem = p3_smem<T, NN>(W, a.g.Mx);
-    static int cache = 0;
-    k_p3<T, NN, W><<<resident_grid(k_p3<T, NN, W>, NTP, p3_smem<T, NN>(W, NN), ntiles, cache), NTP, smem, st>>>(
-        a, nzt, ntiles);
-    return cudaGetLastError();
-  });
-}
-
 template <typename K> cudaError_t max_smem(K kernel, int bytes) {
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
 }
 
+template <typename T, int NN, int W, int NTH> cudaError_t launch_p1_v(const P1Args<T>& a, cudaStream_t st) {
+  static int cache = 0;
+  static bool ready = false;
+  if (!ready) {
+    cudaError_t e = max_smem(k_p1<T, NN, W, NTH>, (int)p1_smem<T, NN>(W, NN));
+    if (e != cudaSuccess) return e;
+    ready = true;
+  }
+  const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
+  const size_t smem = p1_smem<T, NN>(W, a.g.Mx);
+  k_p1<T, NN, W, NTH><<<resident_grid(k_p1<T, NN, W, NTH>, NTH, p1_smem<T, NN>(W, NN), ntiles, cache), NTH, smem,
+                        st>>>(a, nzt, ntiles);
+  return cudaGetLastError();
+}
+
+template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Args<T>& a, cudaStream_t st) {
+  static int cache = 0;
+  static bool ready = false;
+  if (!ready) {
+    cudaError_t e = max_smem(k_p3<T, NN, W, NTH>, (int)p3_smem<T, NN>(W, NN));
+    if (e != cudaSuccess) return e;
+    ready = true;
+  }
+  const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
+  const size_t smem = p3_smem<T, NN>(W, a.g.Mx);
+  k_p3<T, NN, W, NTH><<<resident_grid(k_p3<T, NN, W, NTH>, NTH, p3_smem<T, NN>(W, NN), ntiles, cache), NTH, smem,
+                        st>>>(a, nzt, ntiles);
+  return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st) {
+  return dispatch_len(a.g.Nx, [&](auto nn) {
+    constexpr int NN = decltype(nn)::value;
+    return launch_p1_v<T, NN, tile_wp<T>(NN), NTP>(a, st);
+  });
+}
+
+template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st) {
+  return dispatch_len(a.g.Nx, [&](auto nn) {
+    constexpr int NN = decltype(nn)::value;
+    return launch_p3_v<T, NN, tile_wp<T>(NN), NTP>(a, st);
+  });
+}
+
 template <typename T> cudaError_t prepare_axis_kernels(int Nx) {
   return dispatch_len(Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
-    constexpr int WP = tile_wp<T>(NN);
-    cudaError_t e = max_smem(k_p1<T, NN, WP>, (int)p1_smem<T, NN>(WP, NN));  // upper bounds (Mx <= N)
-    if (e != cudaSuccess) return e;
-    if ((e = max_smem(k_p3<T, NN, WP>, (int)p3_smem<T, NN>(WP, NN))) != cudaSuccess) return e;
+    cudaError_t e;
     constexpr int W = tile_w<T>(NN);
     if ((e = max_smem(k_axis<T, NN, W, true, true>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
     if ((e = max_smem(k_axis<T, NN, W, false, true>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;

@@ -15,7 +15,6 @@
 // first stage forms u x w from them; its last stage leaves the spectrum in
 // shared memory for the r2c post-processing, which writes the three products
 // over the first three input components of the same rows.
-#include <cstdlib>
 #include <type_traits>
 
 #include "fft_core.cuh"
@@ -24,7 +23,7 @@
 namespace hit {
 
 template <int H> __host__ __device__ constexpr int z_rows_per_block() {
-  return (1024 / H) > 32 ? 32 : (1024 / H < 1 ? 1 : 1024 / H);
+  return (512 / H) > 32 ? 32 : (512 / H < 1 ? 1 : 512 / H);
 }
 // threads per block: one per last-stage butterfly of the 3*RB forward rows
 template <int H> __host__ __device__ constexpr int z_threads() {
@@ -80,11 +79,10 @@ template <typename T, int H, int RB, int NTZ, int MINB>
 __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using AD = SkewAddr<skew_ld(H)>;
-  constexpr int KC = z_row_cap<H>();  // >= Mzp: slots per staged row
   V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);  // 6*RB columns of AD::LD slots
   V2<T>* tws = buf + 6 * RB * AD::LD;
   const V2<T>* twz = tws + tw_size<true>(H);
-  V2<T>* raw = tws + z_tw_slots<H>();  // next group's input rows: [q*RB + lr][KC]
+  V2<T>* raw = tws + z_tw_slots<H>();  // next group's input rows: [q*RB + lr][Mzp]
   fill_z_twiddles<T, H, NTZ>(tws, a.tw);
   const int ngroups = (a.nrows + RB - 1) / RB;
   const int Mz = a.Mz, Mzp = a.Mzp;
@@ -97,7 +95,7 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
     for (int e = threadIdx.x; e < 6 * RB * chunks; e += NTZ) {
       const int col = e / chunks, ch = e % chunks;
       const int q = col / RB, lr = col % RB;
-      V2<T>* dst = raw + col * KC + ch * VPC;
+      V2<T>* dst = raw + col * Mzp + ch * VPC;
       if (r0 + lr < a.nrows) cp_async16(dst, a.buf + q * a.c_stride + (r0 + lr) * Mzp + ch * VPC);
       else
         for (int i = 0; i < VPC; ++i) dst[i] = czero<T>();
@@ -120,7 +118,7 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
     fft_ip<T, H, 6 * RB, NTZ, AD, true>(
         buf, tws,
         [&](int k, int col) {
-          const V2<T>* row = raw + col * KC;
+          const V2<T>* row = raw + col * Mzp;
           V2<T> X = k < Mz ? row[k] : czero<T>();
           const int kk = H - k;
           V2<T> Y = kk < Mz ? row[kk] : czero<T>();
@@ -155,13 +153,12 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
         },
         [&](int k, int col, V2<T> v) { buf[AD::at(k, col)] = v; });
 
-    for (int e = threadIdx.x; e < 3 * RB * KC; e += NTZ) {
-      const int col = e / KC, k = e % KC;
+    for (int col = threadIdx.x / 32; col < 3 * RB; col += NTZ / 32) {
       const int q = col / RB, lr = col % RB;
-      if ((full || row0 + lr < a.nrows) && k < Mzp) {
-        V2<T> v = czero<T>();
-        if (k < Mz) v = r2c_post<T>([&](int i) { return buf[AD::at(i, col)]; }, k, H, twz);
-        a.buf[q * a.c_stride + (row0 + lr) * Mzp + k] = v;
+      if (full || row0 + lr < a.nrows) {
+        V2<T>* out = a.buf + q * a.c_stride + (row0 + lr) * Mzp;
+        for (int k = threadIdx.x % 32; k < Mzp; k += 32)
+          out[k] = k < Mz ? r2c_post<T>([&](int i) { return buf[AD::at(i, col)]; }, k, H, twz) : czero<T>();
       }
     }
     __syncthreads();  // buf is rewritten by the next group
@@ -256,20 +253,9 @@ template <typename T, int HH, int RB, int NTZ, int MINB> cudaError_t launch_zcro
 }
 
 template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, cudaStream_t st) {
-  static int cfg = [] { const char* e = getenv("HIT_ZCFG"); return e ? atoi(e) : 0; }();
-  if (H == 256) {
-    switch (cfg) {
-      case 1: return launch_zcross_v<T, 256, 1, 32, 1>(a, st);
-      case 2: return launch_zcross_v<T, 256, 2, 64, 1>(a, st);
-      case 3: return launch_zcross_v<T, 256, 4, 384, 1>(a, st);
-      case 4: return launch_zcross_v<T, 256, 2, 96, 1>(a, st);
-      default: break;
-    }
-  }
   return dispatch_half(H, [&](auto hh) {
     constexpr int HH = decltype(hh)::value;
-    constexpr int RB = z_rows_per_block<HH>();
-    return launch_zcross_v<T, HH, RB, z_threads<HH>(), 2>(a, st);
+    return launch_zcross_v<T, HH, z_rows_per_block<HH>(), z_threads<HH>(), 4>(a, st);
   });
 }
 
