@@ -180,8 +180,22 @@ struct NoHook {
   __device__ void operator()() const {}
 };
 
+// Column-tile slot of (pos, col) for W-wide rows: rows are swizzled by
+// flipping their parity on bit log2(R0) of the position (R0 = radix of the
+// first stage), so the first stage's stride-R0 row stores of the four row
+// groups a warp touches fall into both halves of the banks.
+template <int W, int R0> struct ColSwz {
+  static __device__ __forceinline__ int at(int pos, int col) {
+    constexpr int SH = R0 >= 8 ? 3 : (R0 >= 4 ? 2 : 1);
+    return (pos ^ ((pos >> SH) & 1)) * W + col;
+  }
+};
+template <int SP, int SC> struct Strided {
+  static __device__ __forceinline__ int at(int pos, int col) { return pos * SP + col * SC; }
+};
+
 // One Stockham stage.  SRC/DST: 0 = functor, 1 = buffer A, 2 = buffer B.
-template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, int R, int P, int TWO, int SRC, int DST,
+template <typename T, int N, int NCOLS, int NT, class ADDR, bool INV, int R, int P, int TWO, int SRC, int DST,
           class LD, class ST>
 __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __restrict__ B,
                                              const V2<T>* __restrict__ tws, LD& ld, ST& st) {
@@ -199,7 +213,7 @@ __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __res
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if constexpr (SRC == 0) v[r] = ld(b + r * NB, col);
-        else v[r] = src[(b + r * NB) * SP + col * SC];
+        else v[r] = src[ADDR::at(b + r * NB, col)];
       }
       const int k = b & (P - 1);
       if (P > 1) {
@@ -215,32 +229,32 @@ __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __res
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if constexpr (DST == 0) st(j + r * P, col, v[r]);
-        else dst[(j + r * P) * SP + col * SC] = v[r];
+        else dst[ADDR::at(j + r * P, col)] = v[r];
       }
     }
   }
   if (DST != 0) __syncthreads();
 }
 
-template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, int S, class LD, class ST, class HK>
+template <typename T, int N, int NCOLS, int NT, class ADDR, bool INV, int S, class LD, class ST, class HK>
 __device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* tws, LD& ld, ST& st, HK& hk) {
   constexpr int NS = fft_nstages(N);
   if constexpr (S < NS) {
     constexpr int SRC = S == 0 ? 0 : ((S - 1) % 2 == 0 ? 1 : 2);
     constexpr int DST = S == NS - 1 ? 0 : (S % 2 == 0 ? 1 : 2);
-    fft_stage_io<T, N, NCOLS, NT, SP, SC, INV, fft_radix(N, S), fft_pprod(N, S), tw_offset<false>(N, S), SRC, DST>(
+    fft_stage_io<T, N, NCOLS, NT, ADDR, INV, fft_radix(N, S), fft_pprod(N, S), tw_offset<false>(N, S), SRC, DST>(
         A, B, tws, ld, st);
     if constexpr (S == 0 && !std::is_same<HK, NoHook>::value) {
       if constexpr (DST == 0) __syncthreads();
       hk();
     }
-    fft_stages_io<T, N, NCOLS, NT, SP, SC, INV, S + 1>(A, B, tws, ld, st, hk);
+    fft_stages_io<T, N, NCOLS, NT, ADDR, INV, S + 1>(A, B, tws, ld, st, hk);
   }
 }
 
 // Unnormalised FFT of NCOLS sequences of length N: inputs from ld(pos, col),
 // outputs to st(pos, col, v), intermediate stages in A/B (N*NCOLS elements
-// each, laid out pos*SP + col*SC), twiddles from the shared stage tables tws
+// each, slot ADDR::at(pos, col)), twiddles from the shared stage tables tws
 // (fill_stage_twiddles<T, N, false>).  INV selects exp(+2 pi i nk/N).  The caller
 // synchronises before ld reads shared memory written by other threads and
 // after st writes shared memory that other threads read.  The storer may write
@@ -248,12 +262,14 @@ __device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* t
 // read.
 // after_stage0() (optional) runs once every thread has finished the first
 // stage, when the loader's source may be reused.
-template <typename T, int N, int NCOLS, int NT, int SP, int SC, bool INV, class LD, class ST, class HK = NoHook>
+template <typename T, int N, int NCOLS, int NT, class ADDR, bool INV, class LD, class ST, class HK = NoHook>
 __device__ __forceinline__ void fft_io(V2<T>* A, V2<T>* B, const V2<T>* tws, LD&& ld, ST&& st,
                                        HK&& after_stage0 = HK{}) {
   static_assert((N & (N - 1)) == 0 && N >= 2 && N <= TWN, "power-of-two length");
-  fft_stages_io<T, N, NCOLS, NT, SP, SC, INV, 0>(A, B, tws, ld, st, after_stage0);
+  fft_stages_io<T, N, NCOLS, NT, ADDR, INV, 0>(A, B, tws, ld, st, after_stage0);
 }
+// column tiles of W contiguous columns: swizzled rows
+template <int N, int W> using TileAddr = ColSwz<W, fft_radix(N, 0)>;
 
 // ---------------------------------------------------------------------------
 // In-place variant for row FFTs: one shared buffer; each stage loads all of a

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
       __syncthreads();
     }
     const int nxt = tile + gridDim.x;
-    fft_io<T, N, W, NT, W, 1, INV>(
+    fft_io<T, N, W, NT, TileAddr<N, W>, INV>(
         A, B, tws,
         [&](int pos, int col) {
           const int row = compact_row(pos, a.hin, a.Min, N);
@@ -93,7 +93,7 @@ __device__ __forceinline__ void p1_body(const V2<T>* S, V2<T>* A, V2<T>* B, int 
   const int MW = g.Mx * W;
 #pragma unroll 1
   for (int q = 0; q < 6; ++q) {
-    fft_io<T, N, W, NTH, W, 1, true>(
+    fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
         A, B, tws,
         [&](int pos, int col) {
           const int row = compact_row(pos, g.hx, g.Mx, N);
@@ -186,7 +186,7 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     __syncthreads();
     // once the first stage has read the staged column, stage the next one:
     // component c+1 of this tile, or component 0 of the next tile
-    fft_io<T, N, W, NTH, W, 1, false>(
+    fft_io<T, N, W, NTH, TileAddr<N, W>, false>(
         A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; },
         [&](int pos, int col, V2<T> v) {
           const int row = compact_row(pos, g.hx, g.Mx, N);
@@ -204,97 +204,124 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
   const T cf = (a.forcing == 2 || a.forcing == 3) ? T(a.coef[0]) : T(0);
   double sE = 0.0, sO = 0.0, sB = 0.0;
   const long long cbase = (long long)j * g.Mzp + z0;
-  for (int e = threadIdx.x; e < MW; e += NTH) {
-    const int i = e / W, col = e % W, z = z0 + col;
-    const int pos = full_pos(i, g.hx, g.Mx, N);
-    V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
-    if (z < g.Mz) {
-      const long long idx = cbase + (long long)i * a.c_x + col;
-      const T kx = a.k.kx[pos], kz = a.k.kz[z];
-      const T k2 = k2_of(kx, ky, kz);
-      const T ik2 = inv_k2_of(k2);
-      const V2<T>* us_src = a.stage <= 1 ? a.u : a.s;
-      V2<T> us[3], du[3];
+  V2<T>* __restrict__ pu = a.u;
+  V2<T>* __restrict__ pacc = a.acc;
+  V2<T>* __restrict__ ps = a.s;
+  V2<T>* __restrict__ pout = a.out;
+  const V2<T>* __restrict__ pus = a.stage <= 1 ? a.u : a.s;
+  const int stage = a.stage;
+  // two elements per pass: all their state loads are in flight together
+  for (int e0 = threadIdx.x; e0 < MW; e0 += 2 * NTH) {
+    V2<T> us[2][3], ac[2][3], uu[2][3];
+    long long idx[2];
+    bool ok[2];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        us[c] = us_src[c * a.c_c + idx];
-        du[c] = F[c * MW + e];
-      }
-      // forcing term, added before dealias and projection (navierstokes.py:88-92)
-      if (a.forcing == 1) {
+    for (int h = 0; h < 2; ++h) {
+      const int e = e0 + h * NTH;
+      const int i = e / W, col = e % W;
+      ok[h] = e < MW && z0 + col < g.Mz;
+      idx[h] = cbase + (long long)i * a.c_x + col;
+      if (ok[h]) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], a.fA));
-      } else if (a.forcing == 2) {
-        if (a.kmin2 <= k2 && k2 <= a.kmax2) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], cf));
+        for (int c = 0; c < 3; ++c) {
+          us[h][c] = pus[c * a.c_c + idx[h]];
+          if (stage >= 2) {
+            ac[h][c] = pacc[c * a.c_c + idx[h]];
+            uu[h][c] = pu[c * a.c_c + idx[h]];
+          }
         }
-      } else if (a.forcing == 3) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], cf));
-      }
-      if (!in_dealias(g, pos, fy, z)) {
-        du[0] = du[1] = du[2] = czero<T>();
-      }
-      // projection: div = (kx d0 + ky d1 + kz d2) / k^2 ; d -= k div
-      V2<T> div;
-      div.x = (kx * du[0].x + ky * du[1].x + kz * du[2].x) * ik2;
-      div.y = (kx * du[0].y + ky * du[1].y + kz * du[2].y) * ik2;
-      du[0] = csub(du[0], cscale(div, kx));
-      du[1] = csub(du[1], cscale(div, ky));
-      du[2] = csub(du[2], cscale(div, kz));
-      const T nk2 = a.nu * k2;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) du[c] = csub(du[c], cscale(us[c], nk2));
-
-      const long long o = idx;
-      switch (a.stage) {
-        case 0:
-#pragma unroll
-          for (int c = 0; c < 3; ++c) a.out[c * a.c_c + o] = du[c];
-          break;
-        case 1:
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            a.acc[c * a.c_c + o] = du[c];
-            ns[c] = cadd(us[c], cscale(du[c], a.a_next));
-            a.s[c * a.c_c + o] = ns[c];
-          }
-          break;
-        case 2:
-        case 3:
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            V2<T> ac = a.acc[c * a.c_c + o];
-            ac.x = ac.x + T(2) * du[c].x;
-            ac.y = ac.y + T(2) * du[c].y;
-            a.acc[c * a.c_c + o] = ac;
-            ns[c] = cadd(a.u[c * a.c_c + o], cscale(du[c], a.a_next));
-            a.s[c * a.c_c + o] = ns[c];
-          }
-          break;
-        default:
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const V2<T> ac = cadd(a.acc[c * a.c_c + o], du[c]);
-            ns[c] = cadd(a.u[c * a.c_c + o], cscale(ac, a.dt6));
-            a.u[c * a.c_c + o] = ns[c];
-          }
-          break;
-      }
-      if (a.partial) {
-        double a2 = 0.0;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) a2 += (double)ns[c].x * ns[c].x + (double)ns[c].y * ns[c].y;
-        const double w = herm_weight(g, z);
-        sE += w * a2;
-        sO += w * (double)k2 * a2;
-        if (a.kmin2 <= k2 && k2 <= a.kmax2) sB += w * a2;
       }
     }
-    if (a.fuse_p1) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) F[c * MW + e] = ns[c];
+    for (int h = 0; h < 2; ++h) {
+      const int e = e0 + h * NTH;
+      if (e >= MW) continue;
+      const int i = e / W, col = e % W, z = z0 + col;
+      const int pos = full_pos(i, g.hx, g.Mx, N);
+      V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
+      if (ok[h]) {
+        const long long o = idx[h];
+        const T kx = a.k.kx[pos], kz = a.k.kz[z];
+        const T k2 = k2_of(kx, ky, kz);
+        const T ik2 = inv_k2_of(k2);
+        V2<T> du[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) du[c] = F[c * MW + e];
+        // forcing term, added before dealias and projection (navierstokes.py:88-92)
+        if (a.forcing == 1) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[h][c], a.fA));
+        } else if (a.forcing == 2) {
+          if (a.kmin2 <= k2 && k2 <= a.kmax2) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[h][c], cf));
+          }
+        } else if (a.forcing == 3) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[h][c], cf));
+        }
+        if (!in_dealias(g, pos, fy, z)) {
+          du[0] = du[1] = du[2] = czero<T>();
+        }
+        // projection: div = (kx d0 + ky d1 + kz d2) / k^2 ; d -= k div
+        V2<T> div;
+        div.x = (kx * du[0].x + ky * du[1].x + kz * du[2].x) * ik2;
+        div.y = (kx * du[0].y + ky * du[1].y + kz * du[2].y) * ik2;
+        du[0] = csub(du[0], cscale(div, kx));
+        du[1] = csub(du[1], cscale(div, ky));
+        du[2] = csub(du[2], cscale(div, kz));
+        const T nk2 = a.nu * k2;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) du[c] = csub(du[c], cscale(us[h][c], nk2));
+
+        switch (stage) {
+          case 0:
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pout[c * a.c_c + o] = du[c];
+            break;
+          case 1:
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              pacc[c * a.c_c + o] = du[c];
+              ns[c] = cadd(us[h][c], cscale(du[c], a.a_next));
+              ps[c * a.c_c + o] = ns[c];
+            }
+            break;
+          case 2:
+          case 3:
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              V2<T> acn = ac[h][c];
+              acn.x = acn.x + T(2) * du[c].x;
+              acn.y = acn.y + T(2) * du[c].y;
+              pacc[c * a.c_c + o] = acn;
+              ns[c] = cadd(uu[h][c], cscale(du[c], a.a_next));
+              ps[c * a.c_c + o] = ns[c];
+            }
+            break;
+          default:
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const V2<T> acn = cadd(ac[h][c], du[c]);
+              ns[c] = cadd(uu[h][c], cscale(acn, a.dt6));
+              pu[c * a.c_c + o] = ns[c];
+            }
+            break;
+        }
+        if (a.partial) {
+          double a2 = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) a2 += (double)ns[c].x * ns[c].x + (double)ns[c].y * ns[c].y;
+          const double w = herm_weight(g, z);
+          sE += w * a2;
+          sO += w * (double)k2 * a2;
+          if (a.kmin2 <= k2 && k2 <= a.kmax2) sB += w * a2;
+        }
+      }
+      if (a.fuse_p1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) F[c * MW + e] = ns[c];
+      }
     }
   }
   if (a.partial) {

@@ -184,6 +184,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--shape", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="anisotropic grid for small profiling cases (overrides --size)")
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -206,7 +208,8 @@ def main():
     h3 = importlib.import_module("3dhit_b200")
     nat = importlib.import_module("3dhit_b200._native")
     N = args.size
-    g = h3.make_grid(N, dtype=torch.float32, device=dev)
+    dims = tuple(args.shape) if args.shape else (N, N, N)
+    g = h3.make_grid(*dims, dtype=torch.float32, device=dev)
     u0 = h3.hit_initial_field(rank, g)
     dt = h3.cfl_dt(u0, g, CFL)
     p = h3.NSParams(nu=NU, forcing=h3.BandForcing(eps=EPS, kmin=KMIN, kmax=KMAX))
@@ -253,7 +256,7 @@ def main():
     prm = h3.forcing.native_params(NU, p.forcing, nat.HIT_FLAG_ASSUME_DEALIASED)
     nat.call("hit_profile_rollout", g.plan.handle, nat.ptr(u), prm, float(dt), args.profile_steps,
              nat.ptr(out), msa, cnt, nat.stream_ptr(dev))
-    alg = kernel_alg_bytes(N)
+    alg = kernel_alg_bytes(N) if not args.shape else {k: 0.0 for k in nat.KERNEL_CLASSES}
     per_kernel = {}
     for i, name in enumerate(nat.KERNEL_CLASSES):
         if cnt[i]:
@@ -261,6 +264,12 @@ def main():
             per_kernel[name] = {"launches": cnt[i], "total_ms": msa[i], "avg_ms": avg,
                                 "alg_bytes": alg[name],
                                 "alg_gbs": alg[name] / (avg / 1000.0) / 1e9 if alg[name] else None}
+    if args.shape:  # profiling case: kernel times only
+        if rank == 0:
+            print(json.dumps({"shape": dims, "ms_per_step": ms_step, "kernels": per_kernel}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     tot = sum(v["total_ms"] for v in per_kernel.values())
     for v in per_kernel.values():
         v["share"] = v["total_ms"] / tot
