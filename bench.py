@@ -39,6 +39,22 @@ WORKLOAD = "band-forced HIT 512^3 fp32 (BandForcing eps=0.1 k=[1,2], nu=6e-4, CF
 NU, EPS, KMIN, KMAX, CFL = 6e-4, 0.1, 1.0, 2.0, 0.5
 
 
+def max_over_ranks(x, dist=None, device=None):
+    """Maximum of a per-rank float over all ranks (the device timing rule:
+    the job is as slow as its slowest rank)."""
+    if dist is None:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, steps, ms_max):
+    """Whole-job steps/s: every rank advances its own replica `steps` steps
+    and the job takes the slowest rank's time."""
+    return world * steps / (ms_max / 1000.0)
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -236,16 +252,12 @@ def main():
     torch.cuda.synchronize()
     barrier()
     ck = clocks.stop() if clocks else None
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     E_end = float(h3.energy(u, g))
     if not np.isfinite(E_end):
         raise RuntimeError("non-finite energy after the timed rollout")
     ms_step = ms_max / args.steps
-    value = world * args.steps / (ms_max / 1000.0)
+    value = job_rate(world, args.steps, ms_max)
     launches_per_step = 1 + 4 * 5  # x-inverse, then 4 x (y-inv, z, y-fwd, x-fwd+epi, coef)
 
     # ---- per-kernel device times (events around every launch) -------------
@@ -309,11 +321,9 @@ def main():
         host_out.copy_(ur, non_blocking=True)
         a1.record(stream)
         torch.cuda.synchronize()
-        te = torch.tensor([a0.elapsed_time(a1)], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te = max_over_ranks(a0.elapsed_time(a1), dist, dev)
         nb = host_in.numel() * host_in.element_size()
-        e2e = {"value": world * args.steps / (float(te.item()) / 1000.0), "unit": "steps/s",
+        e2e = {"value": job_rate(world, args.steps, te), "unit": "steps/s",
                "h2d_bytes_per_step": nb / args.steps, "d2h_bytes_per_step": nb / args.steps,
                "note": f"one public rollout({args.steps} steps) call from pinned host state to pinned host result",
                "wall_s": time.perf_counter() - t0}
