@@ -11,9 +11,10 @@
 //   P1 (x-inverse, k_p1)  -> P2a (y-inverse)  -> P2b (z c2r, u x w, z r2c)
 //   -> P2c (y-forward)    -> P3 (x-forward + forcing/dealias/projection/
 //                              viscous/RK update + next stage's P1)
-// and one RK4 step (src/hit3d/integrators.py:32-38) is P1 plus four such
-// chains, captured once as a CUDA graph and replayed nsteps times (the
-// replacement for lax.scan in rollout, integrators.py:41-53).
+// and one RK4 step (src/hit3d/integrators.py:32-38) is four such chains.  A
+// rollout (integrators.py:41-53, the replacement for lax.scan) runs P1 once,
+// then replays a captured CUDA graph of one step whose last P3 also prepares
+// the next step's P1, and a final graph without that part.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -90,7 +91,7 @@ struct Path {  // one code path: 0 = general (full layout), 1 = dealiased (2/3 b
   bool ready = false;
   Buf t6, u6, U, ACC, S, D, partial, coef;
   int p3_blocks = 0, gather_blocks = 0;
-  cudaGraphExec_t exec = nullptr;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};  // [0]: last step, [1]: step that prepares the next one
   GraphKey key{};
   bool key_valid = false;
 };
@@ -377,14 +378,18 @@ int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt
 }
 
 // One RK4 step on the compact state U (P1 first, then four RHS chains).
+// One RK4 step on the compact state U, starting from the x-inverse of U in T6
+// (left by the previous step's last stage or by a standalone k_p1).  With
+// fuse_next the last stage also runs the x-inverse of the new state for the
+// following step.
 template <typename T>
-int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, cudaStream_t st, Prof* pf = nullptr) {
+int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, bool fuse_next, cudaStream_t st,
+                 Prof* pf = nullptr) {
   int rc;
   const bool red = needs_coef(s.forcing);
-  TIMED(pf, 0, launch_p1_of<T>(p, P, vp<T>(P.U), st));
   for (int stage = 1; stage <= 4; ++stage) {
     if ((rc = launch_p2<T>(p, P, st, pf))) return rc;
-    TIMED(pf, 4, launch_p3_stage<T>(p, P, s, stage, dt, stage < 4, red, st));
+    TIMED(pf, 4, launch_p3_stage<T>(p, P, s, stage, dt, stage < 4 || fuse_next, red, st));
     if (red) TIMED(pf, 5, launch_coef<T>(p, P, s, P.p3_blocks, st));
   }
   return HIT_OK;
@@ -401,8 +406,9 @@ int profile_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
   if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
   Prof pf;
   pf.st = st;
+  TIMED(&pf, 0, launch_p1_of<T>(p, P, vp<T>(P.U), st));
   for (int64_t i = 0; i < nsteps; ++i)
-    if ((rc = enqueue_step<T>(p, P, s, dt, st, &pf))) return rc;
+    if ((rc = enqueue_step<T>(p, P, s, dt, i + 1 < nsteps, st, &pf))) return rc;
   HIT_CK(launch_scatter<T>(vp<T>(P.U), static_cast<V2<T>*>(out), P.g, st));
   HIT_CK(cudaStreamSynchronize(st));
   for (int c = 0; c < HIT_NUM_KERNEL_CLASSES; ++c) {
@@ -449,28 +455,32 @@ int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
   if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
   if (nsteps > 0) {
     const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing};
-    if (!P.exec || !P.key_valid || !(P.key == key)) {
-      if (P.exec) {
-        cudaGraphExecDestroy(P.exec);
-        P.exec = nullptr;
+    if (!P.key_valid || !(P.key == key)) {
+      for (cudaGraphExec_t& ex : P.exec) {
+        if (ex) cudaGraphExecDestroy(ex);
+        ex = nullptr;
       }
       P.key_valid = false;
-      HIT_CK(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
-      rc = enqueue_step<T>(p, P, s, dt, p->cap);
-      cudaGraph_t graph = nullptr;
-      cudaError_t e = cudaStreamEndCapture(p->cap, &graph);
-      if (rc) {
-        if (graph) cudaGraphDestroy(graph);
-        return rc;
+      for (int fused = 0; fused < 2; ++fused) {
+        HIT_CK(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_step<T>(p, P, s, dt, fused == 1, p->cap);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(p->cap, &graph);
+        if (rc) {
+          if (graph) cudaGraphDestroy(graph);
+          return rc;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&P.exec[fused], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
       }
-      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-      e = cudaGraphInstantiate(&P.exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
       P.key = key;
       P.key_valid = true;
     }
-    for (int64_t i = 0; i < nsteps; ++i) HIT_CK(cudaGraphLaunch(P.exec, st));
+    if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
+    for (int64_t i = 0; i + 1 < nsteps; ++i) HIT_CK(cudaGraphLaunch(P.exec[1], st));
+    HIT_CK(cudaGraphLaunch(P.exec[0], st));
   }
   HIT_CK(launch_scatter<T>(vp<T>(P.U), static_cast<V2<T>*>(out), P.g, st));
   return HIT_OK;
@@ -705,7 +715,8 @@ int hit_plan_destroy(hit_plan* p) {
   if (!p) return HIT_OK;
   DeviceGuard dg(p->device);
   for (Path& P : p->path) {
-    if (P.exec) cudaGraphExecDestroy(P.exec);
+    for (cudaGraphExec_t ex : P.exec)
+      if (ex) cudaGraphExecDestroy(ex);
     release(P.t6);
     release(P.u6);
     release(P.U);

@@ -258,7 +258,7 @@ def main():
         raise RuntimeError("non-finite energy after the timed rollout")
     ms_step = ms_max / args.steps
     value = job_rate(world, args.steps, ms_max)
-    launches_per_step = 1 + 4 * 5  # x-inverse, then 4 x (y-inv, z, y-fwd, x-fwd+epi, coef)
+    launches_per_step = 4 * 5  # 4 x (y-inv, z, y-fwd, x-fwd+epi [+ next x-inverse], coef)
 
     # ---- per-kernel device times (events around every launch) -------------
     import ctypes
@@ -343,7 +343,7 @@ def main():
                        "parallelism": f"replicas x{world}", "path": "dealiased (2/3-box transforms)"},
             "grid_point_steps_per_s": value * N**3,
             "roofline": roofline, "step_roofline": step_model, "kernels": per_kernel,
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps + 1,
             "clocks": ck, "energy_end": E_end,
         }
         print(json.dumps(line), flush=True)
