@@ -85,12 +85,6 @@ __device__ __forceinline__ void fill_stage_twiddles(V2<T>* tws, const V2<T>* __r
   }
 }
 
-// Which ping-pong buffer the last stage does not read (0 = A, 1 = B): a
-// caller may let the storer write there.
-__host__ __device__ constexpr int fft_free_buffer(int N) {
-  return fft_nstages(N) < 2 ? 0 : (((fft_nstages(N) - 2) % 2 == 0) ? 1 : 0);
-}
-
 template <bool INV, typename V> __device__ __forceinline__ void dft4(V& x0, V& x1, V& x2, V& x3) {
   V a = cadd(x0, x2), b = csub(x0, x2), c = cadd(x1, x3), d = csub(x1, x3);
   d = INV ? cmul_i(d) : cmul_mi(d);
@@ -180,19 +174,19 @@ struct NoHook {
   __device__ void operator()() const {}
 };
 
-// Column-tile slot of (pos, col) for W-wide rows: rows are swizzled by
-// flipping their parity on bit log2(R0) of the position (R0 = radix of the
-// first stage), so the first stage's stride-R0 row stores of the four row
-// groups a warp touches fall into both halves of the banks.
-template <int W, int R0> struct ColSwz {
-  static __device__ __forceinline__ int at(int pos, int col) {
-    constexpr int SH = R0 >= 8 ? 3 : (R0 >= 4 ? 2 : 1);
-    return (pos ^ ((pos >> SH) & 1)) * W + col;
-  }
+// Column-tile slot of (pos, col) for W-wide rows, with one pad row after every
+// 8 rows.  For every stage of the radix plan, at(b + r*NB) and at(j + r*P) lie
+// at offsets from at(b) and at(j) that depend on r alone (step(r*NB) when NB
+// is a multiple of 8, step(r*P) always), so a thread addresses all its
+// butterfly inputs and outputs from one base slot; and the stride-R rows of the
+// first-stage stores of a warp alternate between the two halves of the banks.
+template <int W> struct Skew8 {
+  static __host__ __device__ constexpr int rows(int N) { return N + (N >> 3); }
+  static __device__ __forceinline__ int at(int pos, int col) { return (pos + (pos >> 3)) * W + col; }
+  static __host__ __device__ constexpr int step(int d) { return (d + (d >> 3)) * W; }
 };
-template <int SP, int SC> struct Strided {
-  static __device__ __forceinline__ int at(int pos, int col) { return pos * SP + col * SC; }
-};
+// Slots of one Skew8 buffer of N-row, W-wide tiles.
+__host__ __device__ constexpr int skew8_slots(int N, int W) { return (N + (N >> 3)) * W; }
 
 // One Stockham stage.  SRC/DST: 0 = functor, 1 = buffer A, 2 = buffer B.
 template <typename T, int N, int NCOLS, int NT, class ADDR, bool INV, int R, int P, int TWO, int SRC, int DST,
@@ -212,8 +206,14 @@ __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __res
       V2<T> v[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        if constexpr (SRC == 0) v[r] = ld(b + r * NB, col);
-        else v[r] = src[ADDR::at(b + r * NB, col)];
+        if constexpr (SRC == 0) {
+          if constexpr (std::is_invocable<LD&, int, int, int>::value) v[r] = ld(b + r * NB, col, r);
+          else v[r] = ld(b + r * NB, col);
+        } else if constexpr (NB % 8 == 0) {
+          v[r] = src[ADDR::at(b, col) + ADDR::step(r * NB)];
+        } else {
+          v[r] = src[ADDR::at(b + r * NB, col)];
+        }
       }
       const int k = b & (P - 1);
       if (P > 1) {
@@ -228,8 +228,12 @@ __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __res
       const int j = (b - k) * R + k;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        if constexpr (DST == 0) st(j + r * P, col, v[r]);
-        else dst[ADDR::at(j + r * P, col)] = v[r];
+        if constexpr (DST == 0) {
+          if constexpr (std::is_invocable<ST&, int, int, V2<T>, int>::value) st(j + r * P, col, v[r], r);
+          else st(j + r * P, col, v[r]);
+        } else {
+          dst[ADDR::at(j, col) + ADDR::step(r * P)] = v[r];
+        }
       }
     }
   }
@@ -253,13 +257,15 @@ __device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* t
 }
 
 // Unnormalised FFT of NCOLS sequences of length N: inputs from ld(pos, col),
-// outputs to st(pos, col, v), intermediate stages in A/B (N*NCOLS elements
-// each, slot ADDR::at(pos, col)), twiddles from the shared stage tables tws
-// (fill_stage_twiddles<T, N, false>).  INV selects exp(+2 pi i nk/N).  The caller
-// synchronises before ld reads shared memory written by other threads and
-// after st writes shared memory that other threads read.  The storer may write
-// into buffer fft_free_buffer(N) (0 = A, 1 = B), which the last stage does not
-// read.
+// outputs to st(pos, col, v), intermediate stages in A/B (ADDR::rows(N)*NCOLS
+// slots each, slot ADDR::at(pos, col)), twiddles from the shared stage tables
+// tws (fill_stage_twiddles<T, N, false>).  INV selects exp(+2 pi i nk/N).  A
+// thread's butterflies are t = threadIdx.x + c*NT (col = t % NCOLS, b = t /
+// NCOLS); ld may take a third argument r and st a fourth, the index of the
+// value within the butterfly (position b + r*N/R in the first stage, j + r*P
+// in the last), so a caller can keep a thread's inputs or outputs in
+// registers.  The caller synchronises before ld reads shared memory written by
+// other threads and after st writes shared memory that other threads read.
 // after_stage0() (optional) runs once every thread has finished the first
 // stage, when the loader's source may be reused.
 template <typename T, int N, int NCOLS, int NT, class ADDR, bool INV, class LD, class ST, class HK = NoHook>
@@ -268,8 +274,8 @@ __device__ __forceinline__ void fft_io(V2<T>* A, V2<T>* B, const V2<T>* tws, LD&
   static_assert((N & (N - 1)) == 0 && N >= 2 && N <= TWN, "power-of-two length");
   fft_stages_io<T, N, NCOLS, NT, ADDR, INV, 0>(A, B, tws, ld, st, after_stage0);
 }
-// column tiles of W contiguous columns: swizzled rows
-template <int N, int W> using TileAddr = ColSwz<W, fft_radix(N, 0)>;
+// column tiles of W contiguous columns
+template <int N, int W> using TileAddr = Skew8<W>;
 
 // ---------------------------------------------------------------------------
 // In-place variant for row FFTs: one shared buffer; each stage loads all of a

@@ -24,14 +24,18 @@
 namespace hit {
 
 // PF: the next tile's stored rows are staged in shared memory with cp.async
-// while the current tile is transformed (needs 16-byte aligned rows/columns).
+// while the current tile is transformed (needs 16-byte aligned rows/columns
+// and whole tiles).  The staging buffer holds all N positions: rows that are
+// not stored stay zero from the kernel start, so the first stage reads it
+// without checks.  The inverse transform always writes all N rows and the
+// forward one always reads all N rows (the launcher checks this).
 template <typename T, int N, int W, bool INV, bool PF>
 __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
-  V2<T>* B = A + N * W;
-  V2<T>* tws = B + N * W;
-  V2<T>* stg = tws + ((tw_size<false>(N) + 1) / 2 * 2);  // PF: Min x W staged rows
+  V2<T>* B = A + skew8_slots(N, W);
+  V2<T>* tws = B + skew8_slots(N, W);
+  V2<T>* stg = tws + ((tw_size<false>(N) + 1) / 2 * 2);  // PF: N x W staged rows
   fill_stage_twiddles<T, N, false, NT>(tws, a.tw);
   constexpr int VPC = 16 / sizeof(V2<T>);
   auto tile_src = [&](int tile) {
@@ -44,11 +48,14 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
     constexpr int CPR = W / VPC;  // 16-byte chunks per row
     for (int e = threadIdx.x; e < a.Min * CPR; e += NT) {
       const int row = e / CPR, ch = e % CPR;
-      cp_async16(stg + row * W + ch * VPC, src + (long long)row * a.s_a + ch * VPC);
+      cp_async16(stg + full_pos(row, a.hin, a.Min, N) * W + ch * VPC, src + (long long)row * a.s_a + ch * VPC);
     }
     cp_async_commit();
   };
-  if (PF && blockIdx.x < ntiles) prefetch(blockIdx.x);
+  if (PF) {
+    for (int e = threadIdx.x; e < (N - a.Min) * W; e += NT) stg[a.hin * W + e] = czero<T>();
+    if (blockIdx.x < ntiles) prefetch(blockIdx.x);
+  }
   __syncthreads();
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int zt = tile % nzt, rest = tile / nzt;
@@ -56,7 +63,7 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
     const long long o = rest % no, c = rest / no;
     const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
     V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
-    const bool zc = z0 + W <= a.nz;  // whole tile inside the valid columns
+    const bool zc = PF || z0 + W <= a.nz;  // whole tile inside the valid columns
     if (PF) {
       cp_async_wait_all();
       __syncthreads();
@@ -65,12 +72,12 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
     fft_io<T, N, W, NT, TileAddr<N, W>, INV>(
         A, B, tws,
         [&](int pos, int col) {
-          const int row = compact_row(pos, a.hin, a.Min, N);
-          if (PF) return row >= 0 ? stg[row * W + col] : czero<T>();
+          if (PF) return stg[pos * W + col];
+          const int row = INV ? compact_row(pos, a.hin, a.Min, N) : pos;
           return (row >= 0 && (zc || z0 + col < a.nz)) ? src[(long long)row * a.s_a + col] : czero<T>();
         },
         [&](int pos, int col, V2<T> v) {
-          const int row = compact_row(pos, a.hout, a.Mout, N);
+          const int row = INV ? pos : compact_row(pos, a.hout, a.Mout, N);
           if (row >= 0 && (zc || z0 + col < a.nz)) dst[(long long)row * a.d_a + col] = v;
         },
         [&]() {
@@ -81,44 +88,51 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
   if (PF) cp_async_wait_all();
 }
 
-// x-inverse of u and w = i k x u for one (ky row, z tile).  S holds the three
-// stage-input columns in compact rows (Mx x W each); A/B are the FFT buffers.
-template <typename T, int N, int W, int NTH>
-__device__ __forceinline__ void p1_body(const V2<T>* S, V2<T>* A, V2<T>* B, int j, int z0, const Geom& g,
+// x-inverse of u and w = i k x u for one (ky row, z tile).  comp(c, pos, col,
+// r) gives component c of the stage input at full x position pos (zero where
+// the position is not stored); r is the index of pos in the calling thread's
+// first-stage butterfly, so a caller may serve it from registers.  The six
+// transforms are unrolled (c is a compile-time index in every call).
+template <typename T, int N, int W, int NTH, class SRC>
+__device__ __forceinline__ void p1_body(SRC&& comp, V2<T>* A, V2<T>* B, int j, int z0, const Geom& g,
                                         const KTab<T>& kt, const V2<T>* tws, V2<T>* t6, long long t_c,
                                         long long t_x) {
   const int fy = full_pos(j, g.hy, g.My, g.Ny);
   const T ky = kt.ky[fy];
   V2<T>* out = t6 + (long long)j * g.Mzp + z0;
-  const int MW = g.Mx * W;
-#pragma unroll 1
-  for (int q = 0; q < 6; ++q) {
+  // w components first, while all three stage-input components are needed;
+  // then u_z, u_x, u_y as their last readers go
+  constexpr int order[6] = {3, 4, 2, 5, 0, 1};
+#pragma unroll
+  for (int qi = 0; qi < 6; ++qi) {
+    const int q = order[qi];
     fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
         A, B, tws,
-        [&](int pos, int col) {
-          const int row = compact_row(pos, g.hx, g.Mx, N);
-          if (row < 0) return czero<T>();
-          const int e = row * W + col;
-          if (q < 3) return S[q * MW + e];
+        [&](int pos, int col, int r) {
+          if (q < 3) return comp(q, pos, col, r);
           const int z = z0 + col;
           const T kx = kt.kx[pos];
           const T kz = z < g.Nzh ? kt.kz[z] : T(0);
-          const V2<T> u0 = S[e], u1 = S[MW + e], u2 = S[2 * MW + e];
           V2<T> d;
           if (q == 3) {
+            const V2<T> u1 = comp(1, pos, col, r), u2 = comp(2, pos, col, r);
             d.x = ky * u2.x - kz * u1.x;
             d.y = ky * u2.y - kz * u1.y;
           } else if (q == 4) {
+            const V2<T> u0 = comp(0, pos, col, r), u2 = comp(2, pos, col, r);
             d.x = kz * u0.x - kx * u2.x;
             d.y = kz * u0.y - kx * u2.y;
           } else {
+            const V2<T> u0 = comp(0, pos, col, r), u1 = comp(1, pos, col, r);
             d.x = kx * u1.x - ky * u0.x;
             d.y = kx * u1.y - ky * u0.y;
           }
           return cmul_i(d);
         },
         [&](int pos, int col, V2<T> v) { out[q * t_c + (long long)pos * t_x + col] = v; });
-    __syncthreads();  // the next transform's first stage rewrites A
+    // an even stage count ends reading A, which the next transform's first
+    // stage rewrites
+    if constexpr (fft_nstages(N) % 2 == 0) __syncthreads();
   }
 }
 
@@ -127,10 +141,15 @@ __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geom& g = a.g;
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
-  V2<T>* B = A + N * W;
-  V2<T>* tws = B + N * W;
-  V2<T>* S = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W
+  V2<T>* B = A + skew8_slots(N, W);
+  V2<T>* tws = B + skew8_slots(N, W);
+  V2<T>* S = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x N x W, rows not stored stay zero
   fill_stage_twiddles<T, N, false, NTH>(tws, a.tw);
+  constexpr int NW = N * W;
+  for (int e = threadIdx.x; e < 3 * (N - g.Mx) * W; e += NTH) {
+    const int c = e / ((N - g.Mx) * W), r = e % ((N - g.Mx) * W);
+    S[c * NW + g.hx * W + r] = czero<T>();
+  }
   const int MW = g.Mx * W;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int j = tile / nzt, z0 = (tile % nzt) * W;
@@ -141,18 +160,142 @@ __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
       for (int e = threadIdx.x; e < 3 * g.Mx; e += NTH)
         prefetch_l2(ns + (e / g.Mx) * a.s_c + (long long)(e % g.Mx) * a.s_x, W * sizeof(V2<T>));
     }
+    __syncthreads();  // the previous tile's transforms have read S
     for (int e = threadIdx.x; e < 3 * MW; e += NTH) {
-      const int c = e / MW, r = e - c * MW;
-      S[e] = src[c * a.s_c + (long long)(r / W) * a.s_x + r % W];
+      const int c = e / MW, r = e - c * MW, i = r / W;
+      S[c * NW + full_pos(i, g.hx, g.Mx, N) * W + r % W] = src[c * a.s_c + (long long)i * a.s_x + r % W];
     }
     __syncthreads();
-    p1_body<T, N, W, NTH>(S, A, B, j, z0, g, a.k, tws, a.t6, a.t_c, a.t_x);
+    p1_body<T, N, W, NTH>([&](int c, int pos, int col, int) { return S[c * NW + pos * W + col]; }, A, B, j, z0, g,
+                          a.k, tws, a.t6, a.t_c, a.t_x);
   }
 }
 
+// Register-resident P3: with a uniform radix-8 plan and one butterfly per
+// thread (N/8 * W == NTH) the forward transform's last stage leaves thread
+// (b, col) holding positions b + r*N/8, exactly the inputs its first inverse
+// stage needs, so the nonlinear term, the epilogue and the new stage input
+// never pass through shared memory.
+template <int N, int W, int NTH> __host__ __device__ constexpr bool p3_in_regs() {
+  return N >= 64 && ilog2(N) % 3 == 0 && (N / 8) * W == NTH;
+}
+
+// State rows of one mode for the epilogue: us = stage input (u for stages
+// 0/1), ac/uu = accumulator and u (stages 2..4).
+template <typename T>
+__device__ __forceinline__ void p3_load(const P3Args<T>& a, long long o, V2<T> (&us)[3], V2<T> (&ac)[3],
+                                        V2<T> (&uu)[3]) {
+  const V2<T>* __restrict__ pus = a.stage <= 1 ? a.u : a.s;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    us[c] = pus[c * a.c_c + o];
+    if (a.stage >= 2) {
+      ac[c] = a.acc[c * a.c_c + o];
+      uu[c] = a.u[c * a.c_c + o];
+    }
+  }
+}
+
+// RHS epilogue of one stored mode (x position pos, z index z, state offset
+// o): du holds the x-forward nonlinear term (u x w)^ on entry.  Forcing is
+// added before dealias and projection (navierstokes.py:88-92), then the
+// viscous term (navierstokes.py:95) and the RK4 stage algebra
+// (integrators.py:32-38); ns receives the new stage input (or new state) and
+// the float64 partial sums are accumulated.
+template <typename T>
+__device__ __forceinline__ void p3_point(const P3Args<T>& a, int pos, int fy, int z, T ky, T cf, long long o,
+                                         V2<T> (&du)[3], const V2<T> (&us)[3], const V2<T> (&ac)[3],
+                                         const V2<T> (&uu)[3], V2<T> (&ns)[3], double& sE, double& sO,
+                                         double& sB) {
+  const Geom& g = a.g;
+  const T kx = a.k.kx[pos], kz = a.k.kz[z];
+  const T k2 = k2_of(kx, ky, kz);
+  const T ik2 = inv_k2_of(k2);
+  if (a.forcing == 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], a.fA));
+  } else if (a.forcing == 2) {
+    if (a.kmin2 <= k2 && k2 <= a.kmax2) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], cf));
+    }
+  } else if (a.forcing == 3) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], cf));
+  }
+  if (!in_dealias(g, pos, fy, z)) {
+    du[0] = du[1] = du[2] = czero<T>();
+  }
+  // projection: div = (kx d0 + ky d1 + kz d2) / k^2 ; d -= k div
+  V2<T> div;
+  div.x = (kx * du[0].x + ky * du[1].x + kz * du[2].x) * ik2;
+  div.y = (kx * du[0].y + ky * du[1].y + kz * du[2].y) * ik2;
+  du[0] = csub(du[0], cscale(div, kx));
+  du[1] = csub(du[1], cscale(div, ky));
+  du[2] = csub(du[2], cscale(div, kz));
+  const T nk2 = a.nu * k2;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) du[c] = csub(du[c], cscale(us[c], nk2));
+
+  V2<T>* __restrict__ pu = a.u;
+  V2<T>* __restrict__ pacc = a.acc;
+  V2<T>* __restrict__ ps = a.s;
+  V2<T>* __restrict__ pout = a.out;
+  switch (a.stage) {
+    case 0:
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        pout[c * a.c_c + o] = du[c];
+        ns[c] = czero<T>();
+      }
+      break;
+    case 1:
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        pacc[c * a.c_c + o] = du[c];
+        ns[c] = cadd(us[c], cscale(du[c], a.a_next));
+        ps[c * a.c_c + o] = ns[c];
+      }
+      break;
+    case 2:
+    case 3:
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        V2<T> acn = ac[c];
+        acn.x = acn.x + T(2) * du[c].x;
+        acn.y = acn.y + T(2) * du[c].y;
+        pacc[c * a.c_c + o] = acn;
+        ns[c] = cadd(uu[c], cscale(du[c], a.a_next));
+        ps[c * a.c_c + o] = ns[c];
+      }
+      break;
+    default:
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const V2<T> acn = cadd(ac[c], du[c]);
+        ns[c] = cadd(uu[c], cscale(acn, a.dt6));
+        pu[c * a.c_c + o] = ns[c];
+      }
+      break;
+  }
+  if (a.partial) {
+    double a2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a2 += (double)ns[c].x * ns[c].x + (double)ns[c].y * ns[c].y;
+    const double w = herm_weight(g, z);
+    sE += w * a2;
+    sO += w * (double)k2 * a2;
+    if (a.kmin2 <= k2 && k2 <= a.kmax2) sB += w * a2;
+  }
+}
+
+// One (ky row, z tile) of P3.  stg holds the staged first nl component of this
+// tile; A/B are the FFT buffers; F (shared-memory mode only) holds the
+// nonlinear term and then the new stage input in compact rows (3 x Mx x W).
 template <typename T, int N, int W, int NTH>
 __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, const V2<T>* tws, V2<T>* F, double* red,
                                         int j, int z0, int tile, V2<T>* stg, int nzt, int ntiles) {
+  constexpr bool REGS = p3_in_regs<N, W, NTH>();
   const Geom& g = a.g;
   const int MW = g.Mx * W;
   constexpr int VPC = 16 / sizeof(V2<T>);
@@ -180,147 +323,88 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     }
   }
 
-#pragma unroll 1
+  // registers of the in-register mode: f[c][r] = component c at position
+  // b + r*N/8 of column col (nl, then the new stage input)
+  V2<T> f[3][REGS ? 8 : 1];
+  const auto nl_store = [&](int c) {
+    return [&, c](int pos, int col, V2<T> v, int r) {
+      if constexpr (REGS) {
+        f[c][r] = v;
+      } else {
+        const int row = compact_row(pos, g.hx, g.Mx, N);
+        if (row >= 0) F[c * MW + row * W + col] = v;
+      }
+    };
+  };
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
     cp_async_wait_all();
     __syncthreads();
     // once the first stage has read the staged column, stage the next one:
     // component c+1 of this tile, or component 0 of the next tile
     fft_io<T, N, W, NTH, TileAddr<N, W>, false>(
-        A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; },
-        [&](int pos, int col, V2<T> v) {
-          const int row = compact_row(pos, g.hx, g.Mx, N);
-          if (row >= 0) F[c * MW + row * W + col] = v;
-        },
+        A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; }, nl_store(c),
         [&]() {
           if (c < 2) prefetch(tile, c + 1, stg);
           else if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, 0, stg);
         });
-    __syncthreads();
   }
+  if constexpr (!REGS) __syncthreads();  // F complete
 
   const int fy = full_pos(j, g.hy, g.My, g.Ny);
   const T ky = a.k.ky[fy];
   const T cf = (a.forcing == 2 || a.forcing == 3) ? T(a.coef[0]) : T(0);
   double sE = 0.0, sO = 0.0, sB = 0.0;
   const long long cbase = (long long)j * g.Mzp + z0;
-  V2<T>* __restrict__ pu = a.u;
-  V2<T>* __restrict__ pacc = a.acc;
-  V2<T>* __restrict__ ps = a.s;
-  V2<T>* __restrict__ pout = a.out;
-  const V2<T>* __restrict__ pus = a.stage <= 1 ? a.u : a.s;
-  const int stage = a.stage;
-  // two elements per pass: all their state loads are in flight together
-  for (int e0 = threadIdx.x; e0 < MW; e0 += 2 * NTH) {
-    V2<T> us[2][3], ac[2][3], uu[2][3];
-    long long idx[2];
-    bool ok[2];
+  if constexpr (REGS) {
+    const int col = threadIdx.x % W, b = threadIdx.x / W;
+    const int z = z0 + col;
+    const bool zok = z < g.Mz;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int e = e0 + h * NTH;
-      const int i = e / W, col = e % W;
-      ok[h] = e < MW && z0 + col < g.Mz;
-      idx[h] = cbase + (long long)i * a.c_x + col;
-      if (ok[h]) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          us[h][c] = pus[c * a.c_c + idx[h]];
-          if (stage >= 2) {
-            ac[h][c] = pacc[c * a.c_c + idx[h]];
-            uu[h][c] = pu[c * a.c_c + idx[h]];
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int e = e0 + h * NTH;
-      if (e >= MW) continue;
-      const int i = e / W, col = e % W, z = z0 + col;
-      const int pos = full_pos(i, g.hx, g.Mx, N);
+    for (int r = 0; r < 8; ++r) {
+      V2<T> us[3], ac[3], uu[3];
+      const int pos = b + r * (N / 8);
+      const int i = compact_row(pos, g.hx, g.Mx, N);
+      const bool ok = zok && i >= 0;
+      const long long o = cbase + (long long)i * a.c_x + col;
+      V2<T> du[3] = {f[0][r], f[1][r], f[2][r]};
       V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
-      if (ok[h]) {
-        const long long o = idx[h];
-        const T kx = a.k.kx[pos], kz = a.k.kz[z];
-        const T k2 = k2_of(kx, ky, kz);
-        const T ik2 = inv_k2_of(k2);
-        V2<T> du[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) du[c] = F[c * MW + e];
-        // forcing term, added before dealias and projection (navierstokes.py:88-92)
-        if (a.forcing == 1) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[h][c], a.fA));
-        } else if (a.forcing == 2) {
-          if (a.kmin2 <= k2 && k2 <= a.kmax2) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[h][c], cf));
-          }
-        } else if (a.forcing == 3) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[h][c], cf));
-        }
-        if (!in_dealias(g, pos, fy, z)) {
-          du[0] = du[1] = du[2] = czero<T>();
-        }
-        // projection: div = (kx d0 + ky d1 + kz d2) / k^2 ; d -= k div
-        V2<T> div;
-        div.x = (kx * du[0].x + ky * du[1].x + kz * du[2].x) * ik2;
-        div.y = (kx * du[0].y + ky * du[1].y + kz * du[2].y) * ik2;
-        du[0] = csub(du[0], cscale(div, kx));
-        du[1] = csub(du[1], cscale(div, ky));
-        du[2] = csub(du[2], cscale(div, kz));
-        const T nk2 = a.nu * k2;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) du[c] = csub(du[c], cscale(us[h][c], nk2));
-
-        switch (stage) {
-          case 0:
-#pragma unroll
-            for (int c = 0; c < 3; ++c) pout[c * a.c_c + o] = du[c];
-            break;
-          case 1:
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              pacc[c * a.c_c + o] = du[c];
-              ns[c] = cadd(us[h][c], cscale(du[c], a.a_next));
-              ps[c * a.c_c + o] = ns[c];
-            }
-            break;
-          case 2:
-          case 3:
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              V2<T> acn = ac[h][c];
-              acn.x = acn.x + T(2) * du[c].x;
-              acn.y = acn.y + T(2) * du[c].y;
-              pacc[c * a.c_c + o] = acn;
-              ns[c] = cadd(uu[h][c], cscale(du[c], a.a_next));
-              ps[c * a.c_c + o] = ns[c];
-            }
-            break;
-          default:
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              const V2<T> acn = cadd(ac[h][c], du[c]);
-              ns[c] = cadd(uu[h][c], cscale(acn, a.dt6));
-              pu[c * a.c_c + o] = ns[c];
-            }
-            break;
-        }
-        if (a.partial) {
-          double a2 = 0.0;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) a2 += (double)ns[c].x * ns[c].x + (double)ns[c].y * ns[c].y;
-          const double w = herm_weight(g, z);
-          sE += w * a2;
-          sO += w * (double)k2 * a2;
-          if (a.kmin2 <= k2 && k2 <= a.kmax2) sB += w * a2;
-        }
+      if (ok) {
+        p3_load(a, o, us, ac, uu);
+        p3_point(a, pos, fy, z, ky, cf, o, du, us, ac, uu, ns, sE, sO, sB);
       }
-      if (a.fuse_p1) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) F[c * MW + e] = ns[c];
+      for (int c = 0; c < 3; ++c) f[c][r] = ns[c];
+    }
+  } else {
+    // two elements per pass: all their state loads are in flight together
+    for (int e0 = threadIdx.x; e0 < MW; e0 += 2 * NTH) {
+      V2<T> us[2][3], ac[2][3], uu[2][3];
+      long long idx[2];
+      bool ok[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int e = e0 + h * NTH;
+        const int i = e / W, col = e % W;
+        ok[h] = e < MW && z0 + col < g.Mz;
+        idx[h] = cbase + (long long)i * a.c_x + col;
+        if (ok[h]) p3_load(a, idx[h], us[h], ac[h], uu[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int e = e0 + h * NTH;
+        if (e >= MW) continue;
+        const int i = e / W, col = e % W;
+        V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
+        if (ok[h]) {
+          V2<T> du[3] = {F[e], F[MW + e], F[2 * MW + e]};
+          p3_point(a, full_pos(i, g.hx, g.Mx, N), fy, z0 + col, ky, cf, idx[h], du, us[h], ac[h], uu[h], ns, sE,
+                   sO, sB);
+        }
+        if (a.fuse_p1) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) F[c * MW + e] = ns[c];
+        }
       }
     }
   }
@@ -333,8 +417,20 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     r = block_sum_f64(sB, red);
     if (threadIdx.x == 0) a.partial[3 * b + 2] = r;
   }
-  __syncthreads();  // F complete; A/B free for the next tile or the fused x-inverse
-  if (a.fuse_p1) p1_body<T, N, W, NTH>(F, A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x);
+  if constexpr (REGS) {
+    if (a.fuse_p1)
+      p1_body<T, N, W, NTH>([&](int c, int, int, int r) { return f[c][r]; }, A, B, j, z0, g, a.k, tws, a.t6, a.t6_c,
+                            a.t6_x);
+  } else {
+    __syncthreads();  // F complete; A/B free for the next tile or the fused x-inverse
+    if (a.fuse_p1)
+      p1_body<T, N, W, NTH>(
+          [&](int c, int pos, int col, int) {
+            const int row = compact_row(pos, g.hx, g.Mx, N);
+            return row >= 0 ? F[c * MW + row * W + col] : czero<T>();
+          },
+          A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x);
+  }
 }
 
 template <typename T, int N, int W, int NTH>
@@ -342,10 +438,10 @@ __global__ void __launch_bounds__(NTH) k_p3(P3Args<T> a, int nzt, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
-  V2<T>* B = A + N * W;
-  V2<T>* stg = B + N * W;  // staged N x W column of the next nl component
+  V2<T>* B = A + skew8_slots(N, W);
+  V2<T>* stg = B + skew8_slots(N, W);  // staged N x W column of the next nl component
   V2<T>* tws = stg + N * W;
-  V2<T>* F = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W: nl, then the new stage input
+  V2<T>* F = tws + (tw_size<false>(N) + 1) / 2 * 2;  // shared-memory mode: 3 x Mx x W
   fill_stage_twiddles<T, N, false, NTH>(tws, a.tw);
   if (blockIdx.x < ntiles) {
     const int jj = blockIdx.x / nzt, zz = (blockIdx.x % nzt) * W;
@@ -383,17 +479,20 @@ template <typename F> cudaError_t dispatch_len(int N, F&& f) {
   }
 }
 
-// P1/P3 shared memory: A, B (N x W each) and the 3 compact tiles (Mx x W).
-// (twiddle slots rounded to an even count keep what follows 16-byte aligned)
+// P1 shared memory: A, B, the twiddles and the 3 staged components (N x W
+// each); P3: A, B, the staged nl column (N x W), the twiddles and, in
+// shared-memory mode, the 3 compact tiles (Mx x W).  (Twiddle slots rounded to
+// an even count keep what follows 16-byte aligned.)
 template <int N> constexpr int tw_slots_even() { return (tw_size<false>(N) + 1) / 2 * 2; }
-template <typename T, int N> size_t p1_smem(int W, int Mx) {
-  return sizeof(V2<T>) * ((size_t)(2 * N + 3 * Mx) * W + tw_slots_even<N>());
+template <typename T, int N> size_t p1_smem(int W) {
+  return sizeof(V2<T>) * ((size_t)2 * skew8_slots(N, W) + 3 * N * W + tw_slots_even<N>());
 }
-template <typename T, int N> size_t p3_smem(int W, int Mx) {
-  return sizeof(V2<T>) * ((size_t)(3 * N + 3 * Mx) * W + tw_slots_even<N>());
+template <typename T, int N, int W, int NTH> size_t p3_smem(int Mx) {
+  const size_t f = p3_in_regs<N, W, NTH>() ? 0 : (size_t)3 * Mx * W;
+  return sizeof(V2<T>) * ((size_t)2 * skew8_slots(N, W) + N * W + tw_slots_even<N>() + f);
 }
 template <typename T, int N, int W, bool PF> constexpr size_t axis_smem() {
-  return sizeof(V2<T>) * ((PF ? 3 : 2) * N * W + tw_slots_even<N>());
+  return sizeof(V2<T>) * (2 * skew8_slots(N, W) + (PF ? N * W : 0) + tw_slots_even<N>());
 }
 
 template <typename T>
@@ -402,6 +501,7 @@ cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, 
     constexpr int NN = decltype(nn)::value;
     constexpr int W = tile_w<T>(NN);
     const long long ntiles = (long long)nzt * no * nc;
+    if ((inv ? a.Mout : a.Min) != NN) return cudaErrorInvalidValue;  // the full side is all N rows
     // staging needs 16-byte aligned rows and whole tiles
     const bool pf = (sizeof(V2<T>) == 16 || ((a.s_a | a.s_o | a.s_c) % 2 == 0 &&
                                               ((uintptr_t)a.src % 16) == 0)) &&
@@ -452,14 +552,14 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p1_v(const P1Ar
   static int cache = 0;
   static bool ready = false;
   if (!ready) {
-    cudaError_t e = max_smem(k_p1<T, NN, W, NTH>, (int)p1_smem<T, NN>(W, NN));
+    cudaError_t e = max_smem(k_p1<T, NN, W, NTH>, (int)p1_smem<T, NN>(W));
     if (e != cudaSuccess) return e;
     ready = true;
   }
   const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
-  const size_t smem = p1_smem<T, NN>(W, a.g.Mx);
-  k_p1<T, NN, W, NTH><<<resident_grid(k_p1<T, NN, W, NTH>, NTH, p1_smem<T, NN>(W, NN), ntiles, cache), NTH, smem,
-                        st>>>(a, nzt, ntiles);
+  const size_t smem = p1_smem<T, NN>(W);
+  k_p1<T, NN, W, NTH><<<resident_grid(k_p1<T, NN, W, NTH>, NTH, smem, ntiles, cache), NTH, smem, st>>>(a, nzt,
+                                                                                                        ntiles);
   return cudaGetLastError();
 }
 
@@ -467,14 +567,14 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Ar
   static int cache = 0;
   static bool ready = false;
   if (!ready) {
-    cudaError_t e = max_smem(k_p3<T, NN, W, NTH>, (int)p3_smem<T, NN>(W, NN));
+    cudaError_t e = max_smem(k_p3<T, NN, W, NTH>, (int)p3_smem<T, NN, W, NTH>(NN));
     if (e != cudaSuccess) return e;
     ready = true;
   }
   const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
-  const size_t smem = p3_smem<T, NN>(W, a.g.Mx);
-  k_p3<T, NN, W, NTH><<<resident_grid(k_p3<T, NN, W, NTH>, NTH, p3_smem<T, NN>(W, NN), ntiles, cache), NTH, smem,
-                        st>>>(a, nzt, ntiles);
+  const size_t smem = p3_smem<T, NN, W, NTH>(a.g.Mx);
+  k_p3<T, NN, W, NTH><<<resident_grid(k_p3<T, NN, W, NTH>, NTH, p3_smem<T, NN, W, NTH>(NN), ntiles, cache), NTH,
+                        smem, st>>>(a, nzt, ntiles);
   return cudaGetLastError();
 }
 
