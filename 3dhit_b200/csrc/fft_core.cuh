@@ -61,27 +61,18 @@ template <bool PLAN16> __host__ __device__ constexpr int tw_size(int N) {
   return plan_nstages<PLAN16>(N) < 2 ? 1 : tw_offset<PLAN16>(N, plan_nstages<PLAN16>(N));
 }
 // Fill the tables from the global exp(-2 pi i m / TWN) table (all threads call;
-// the caller synchronises before first use).
-template <typename T, int N, bool PLAN16, int NTH>
+// the caller synchronises before first use).  Stage by stage, with the
+// stage's radix, stride and offset as compile-time constants.
+template <typename T, int N, bool PLAN16, int NTH, int S = 1>
 __device__ __forceinline__ void fill_stage_twiddles(V2<T>* tws, const V2<T>* __restrict__ tw) {
-  constexpr int NS = plan_nstages<PLAN16>(N);
-  if constexpr (NS >= 2) {
-    for (int e = threadIdx.x; e < tw_size<PLAN16>(N); e += NTH) {
-      int s = 1;
-#pragma unroll
-      for (int q = 2; q < NS; ++q)
-        if (e >= tw_offset<PLAN16>(N, q)) s = q;
-      int R = 0, P = 0;
-#pragma unroll
-      for (int q = 1; q < NS; ++q)
-        if (q == s) {
-          R = plan_radix<PLAN16>(N, q);
-          P = plan_pprod<PLAN16>(N, q);
-        }
-      const int rel = e - tw_offset<PLAN16>(N, s);
-      const int r = rel / P + 1, k = rel % P;
-      tws[e] = tw[r * k * (TWN / (P * R))];
+  if constexpr (S < plan_nstages<PLAN16>(N)) {
+    constexpr int R = plan_radix<PLAN16>(N, S), P = plan_pprod<PLAN16>(N, S);
+    constexpr int OFF = tw_offset<PLAN16>(N, S), STEP = TWN / (P * R);
+    for (int e = threadIdx.x; e < (R - 1) * P; e += NTH) {
+      const int r = e / P + 1, k = e % P;
+      tws[OFF + e] = tw[r * k * STEP];
     }
+    fill_stage_twiddles<T, N, PLAN16, NTH, S + 1>(tws, tw);
   }
 }
 

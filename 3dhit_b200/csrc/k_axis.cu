@@ -157,14 +157,16 @@ __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
     const int nxt = tile + gridDim.x;
     if (nxt < ntiles) {  // next tile's rows into L2 while this one is transformed
       const V2<T>* ns = a.s + (long long)(nxt / nzt) * g.Mzp + (nxt % nzt) * W;
-      for (int e = threadIdx.x; e < 3 * g.Mx; e += NTH)
-        prefetch_l2(ns + (e / g.Mx) * a.s_c + (long long)(e % g.Mx) * a.s_x, W * sizeof(V2<T>));
+      for (int c = 0; c < 3; ++c)
+        for (int i = threadIdx.x; i < g.Mx; i += NTH)
+          prefetch_l2(ns + c * a.s_c + (long long)i * a.s_x, W * sizeof(V2<T>));
     }
     __syncthreads();  // the previous tile's transforms have read S
-    for (int e = threadIdx.x; e < 3 * MW; e += NTH) {
-      const int c = e / MW, r = e - c * MW, i = r / W;
-      S[c * NW + full_pos(i, g.hx, g.Mx, N) * W + r % W] = src[c * a.s_c + (long long)i * a.s_x + r % W];
-    }
+    for (int c = 0; c < 3; ++c)
+      for (int e = threadIdx.x; e < MW; e += NTH) {
+        const int i = e / W, col = e % W;
+        S[c * NW + full_pos(i, g.hx, g.Mx, N) * W + col] = src[c * a.s_c + (long long)i * a.s_x + col];
+      }
     __syncthreads();
     p1_body<T, N, W, NTH>([&](int c, int pos, int col, int) { return S[c * NW + pos * W + col]; }, A, B, j, z0, g,
                           a.k, tws, a.t6, a.t_c, a.t_x);
@@ -314,12 +316,12 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
   // pull the state rows the epilogue reads into L2 while the forward
   // transforms run (one 16-byte-aligned W-wide row segment per prefetch)
   {
-    const int narr = a.stage <= 1 ? 1 : 3;  // u | s, acc, u
-    const V2<T>* arrs[3] = {a.stage <= 1 ? a.u : a.s, a.acc, a.u};
+    const int nq = a.stage <= 1 ? 3 : 9;  // (array, component): u | s, acc, u
     const long long cbase = (long long)j * g.Mzp + z0;
-    for (int e = threadIdx.x; e < narr * 3 * g.Mx; e += NTH) {
-      const int ar = e / (3 * g.Mx), rem = e % (3 * g.Mx), c = rem / g.Mx, i = rem % g.Mx;
-      prefetch_l2(arrs[ar] + c * a.c_c + (long long)i * a.c_x + cbase, W * sizeof(V2<T>));
+    for (int q = 0; q < nq; ++q) {
+      const V2<T>* arr = q < 3 ? (a.stage <= 1 ? a.u : a.s) : (q < 6 ? a.acc : a.u);
+      const V2<T>* base = arr + (q % 3) * a.c_c + cbase;
+      for (int i = threadIdx.x; i < g.Mx; i += NTH) prefetch_l2(base + (long long)i * a.c_x, W * sizeof(V2<T>));
     }
   }
 

@@ -82,23 +82,36 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);  // 6*RB columns of AD::LD slots
   V2<T>* tws = buf + 6 * RB * AD::LD;
   const V2<T>* twz = tws + tw_size<true>(H);
-  V2<T>* raw = tws + z_tw_slots<H>();  // next group's input rows: [q*RB + lr][Mzp]
+  // next group's input rows [q*RB + lr][RS]: entries past Mzp stay zero, so the
+  // c2r pre-processing reads X[k] and X[H-k] without checks.  Entries Mz..Mzp-1
+  // are the rows' padding columns, which every compact spectral buffer keeps
+  // zero (the gather writes zeros there and no RHS kernel writes anything else).
+  constexpr int RS = z_row_cap<H>();
+  V2<T>* raw = tws + z_tw_slots<H>();
   fill_z_twiddles<T, H, NTZ>(tws, a.tw);
   const int ngroups = (a.nrows + RB - 1) / RB;
-  const int Mz = a.Mz, Mzp = a.Mzp;
+  const int Mzp = a.Mzp;
   constexpr int VPC = 16 / sizeof(V2<T>);  // complex values per 16-byte copy
+  for (int e = threadIdx.x; e < 6 * RB * RS; e += NTZ)
+    if (e % RS >= Mzp) raw[e] = czero<T>();
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  constexpr int NWARP = NTZ / 32;
 
-  // stage the 6 component rows of a group (rows past the end are zero-filled)
+  // stage the 6 component rows of a group (rows past the end are zero-filled):
+  // a warp per row, a lane per 16-byte chunk
   auto prefetch = [&](int grp) {
     const long long r0 = (long long)grp * RB;
     const int chunks = Mzp / VPC;  // Mzp is a multiple of 8: whole 16-byte chunks
-    for (int e = threadIdx.x; e < 6 * RB * chunks; e += NTZ) {
-      const int col = e / chunks, ch = e % chunks;
+    for (int col = warp; col < 6 * RB; col += NWARP) {
       const int q = col / RB, lr = col % RB;
-      V2<T>* dst = raw + col * Mzp + ch * VPC;
-      if (r0 + lr < a.nrows) cp_async16(dst, a.buf + q * a.c_stride + (r0 + lr) * Mzp + ch * VPC);
-      else
-        for (int i = 0; i < VPC; ++i) dst[i] = czero<T>();
+      V2<T>* dst = raw + col * RS;
+      const bool in = r0 + lr < a.nrows;
+      const V2<T>* src = a.buf + q * a.c_stride + (r0 + lr) * Mzp;
+      for (int ch = lane; ch < chunks; ch += 32) {
+        if (in) cp_async16(dst + ch * VPC, src + ch * VPC);
+        else
+          for (int i = 0; i < VPC; ++i) dst[ch * VPC + i] = czero<T>();
+      }
     }
     cp_async_commit();
   };
@@ -118,10 +131,9 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
     fft_ip<T, H, 6 * RB, NTZ, AD, true>(
         buf, tws,
         [&](int k, int col) {
-          const V2<T>* row = raw + col * Mzp;
-          V2<T> X = k < Mz ? row[k] : czero<T>();
-          const int kk = H - k;
-          V2<T> Y = kk < Mz ? row[kk] : czero<T>();
+          const V2<T>* row = raw + col * RS;
+          V2<T> X = row[k];
+          V2<T> Y = row[H - k];
           if (k == 0) {
             X.y = T(0);
             Y.y = T(0);
@@ -153,11 +165,12 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
         },
         [&](int k, int col, V2<T> v) { buf[AD::at(k, col)] = v; });
 
-    for (int col = threadIdx.x / 32; col < 3 * RB; col += NTZ / 32) {
+    const int Mz = a.Mz;
+    for (int col = warp; col < 3 * RB; col += NWARP) {
       const int q = col / RB, lr = col % RB;
       if (full || row0 + lr < a.nrows) {
         V2<T>* out = a.buf + q * a.c_stride + (row0 + lr) * Mzp;
-        for (int k = threadIdx.x % 32; k < Mzp; k += 32)
+        for (int k = lane; k < Mzp; k += 32)
           out[k] = k < Mz ? r2c_post<T>([&](int i) { return buf[AD::at(i, col)]; }, k, H, twz) : czero<T>();
       }
     }
