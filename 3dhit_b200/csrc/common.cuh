@@ -31,6 +31,12 @@ template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
   return r;
 }
 template <typename V, typename T> __device__ __forceinline__ V cscale(V a, T s) { a.x *= s; a.y *= s; return a; }
+// float2: one paired-FP32 instruction (FADD2 / FFMA2 / FMUL2) per complex
+// add, subtract or scale; each component rounds exactly as the scalar
+// operation does (a - b is formed as b * -1 + a, whose product is exact).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 // multiply by +i / -i
 template <typename V> __device__ __forceinline__ V cmul_i(V a) { V r; r.x = -a.y; r.y = a.x; return r; }
 template <typename V> __device__ __forceinline__ V cmul_mi(V a) { V r; r.x = a.y; r.y = -a.x; return r; }

@@ -291,9 +291,17 @@ __device__ __forceinline__ void p3_point(const P3Args<T>& a, int pos, int fy, in
   }
 }
 
+// Register mode: the epilogue runs in 8 passes, pass r over the positions
+// r*N/8 .. r*N/8 + N/8 - 1 (position b + r*N/8 of every thread).  The state
+// rows of a pass (up to 3 arrays x 3 components x N/8 rows x W) are copied to
+// a 3-slot shared-memory ring with cp.async two passes ahead, the first two
+// while the last forward transform runs, so the epilogue reads shared memory.
+template <int N, int W> constexpr int p3_ring_slot() { return 9 * (N / 8) * W; }
+
 // One (ky row, z tile) of P3.  stg holds the staged first nl component of this
-// tile; A/B are the FFT buffers; F (shared-memory mode only) holds the
-// nonlinear term and then the new stage input in compact rows (3 x Mx x W).
+// tile; A/B are the FFT buffers; F holds, in shared-memory mode, the nonlinear
+// term and then the new stage input in compact rows (3 x Mx x W), and in
+// register mode the epilogue's state ring (3 slots of p3_ring_slot).
 template <typename T, int N, int W, int NTH>
 __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, const V2<T>* tws, V2<T>* F, double* red,
                                         int j, int z0, int tile, V2<T>* stg, int nzt, int ntiles) {
@@ -325,6 +333,27 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     }
   }
 
+  // register mode: copy the state rows of epilogue pass r into ring slot r % 3
+  const V2<T>* __restrict__ us_arr = a.stage <= 1 ? a.u : a.s;
+  auto stage_pass = [&](int r) {
+    if constexpr (REGS) {
+      constexpr int NB = N / 8, CPR = W / VPC;
+      const int nq = a.stage <= 1 ? 3 : 9;
+      V2<T>* slot = F + (r % 3) * p3_ring_slot<N, W>();
+      const long long cbase = (long long)j * g.Mzp + z0;
+      for (int e = threadIdx.x; e < nq * NB * CPR; e += NTH) {
+        const int q = e / (NB * CPR), rem = e % (NB * CPR), lr = rem / CPR, ch = rem % CPR;
+        const int i = compact_row(r * NB + lr, g.hx, g.Mx, N);
+        if (i >= 0) {
+          const V2<T>* arr = q < 3 ? us_arr : (q < 6 ? a.acc : a.u);
+          cp_async16(slot + (q * NB + lr) * W + ch * VPC,
+                     arr + (q % 3) * a.c_c + cbase + (long long)i * a.c_x + ch * VPC);
+        }
+      }
+      cp_async_commit();
+    }
+  };
+
   // registers of the in-register mode: f[c][r] = component c at position
   // b + r*N/8 of column col (nl, then the new stage input)
   V2<T> f[3][REGS ? 8 : 1];
@@ -347,8 +376,13 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     fft_io<T, N, W, NTH, TileAddr<N, W>, false>(
         A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; }, nl_store(c),
         [&]() {
-          if (c < 2) prefetch(tile, c + 1, stg);
-          else if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, 0, stg);
+          if (c < 2) {
+            prefetch(tile, c + 1, stg);
+          } else {
+            if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, 0, stg);
+            stage_pass(0);
+            stage_pass(1);
+          }
         });
   }
   if constexpr (!REGS) __syncthreads();  // F complete
@@ -364,6 +398,13 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     const bool zok = z < g.Mz;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
+      // pass r's copies are done (only pass r+1's may be pending) and every
+      // thread has left pass r-1, whose slot now takes pass r+2
+      cp_async_wait_group<1>();
+      __syncthreads();
+      if (r + 2 < 8) stage_pass(r + 2);
+      else cp_async_commit();  // empty group: keeps one group per pass
+      const V2<T>* slot = F + (r % 3) * p3_ring_slot<N, W>() + b * W + col;
       V2<T> us[3], ac[3], uu[3];
       const int pos = b + r * (N / 8);
       const int i = compact_row(pos, g.hx, g.Mx, N);
@@ -372,7 +413,14 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
       V2<T> du[3] = {f[0][r], f[1][r], f[2][r]};
       V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
       if (ok) {
-        p3_load(a, o, us, ac, uu);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          us[c] = slot[c * (N / 8) * W];
+          if (a.stage >= 2) {
+            ac[c] = slot[(3 + c) * (N / 8) * W];
+            uu[c] = slot[(6 + c) * (N / 8) * W];
+          }
+        }
         p3_point(a, pos, fy, z, ky, cf, o, du, us, ac, uu, ns, sE, sO, sB);
       }
 #pragma unroll
@@ -443,7 +491,7 @@ __global__ void __launch_bounds__(NTH) k_p3(P3Args<T> a, int nzt, int ntiles) {
   V2<T>* B = A + skew8_slots(N, W);
   V2<T>* stg = B + skew8_slots(N, W);  // staged N x W column of the next nl component
   V2<T>* tws = stg + N * W;
-  V2<T>* F = tws + (tw_size<false>(N) + 1) / 2 * 2;  // shared-memory mode: 3 x Mx x W
+  V2<T>* F = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W, or the register mode's ring
   fill_stage_twiddles<T, N, false, NTH>(tws, a.tw);
   if (blockIdx.x < ntiles) {
     const int jj = blockIdx.x / nzt, zz = (blockIdx.x % nzt) * W;
@@ -490,7 +538,7 @@ template <typename T, int N> size_t p1_smem(int W) {
   return sizeof(V2<T>) * ((size_t)2 * skew8_slots(N, W) + 3 * N * W + tw_slots_even<N>());
 }
 template <typename T, int N, int W, int NTH> size_t p3_smem(int Mx) {
-  const size_t f = p3_in_regs<N, W, NTH>() ? 0 : (size_t)3 * Mx * W;
+  const size_t f = p3_in_regs<N, W, NTH>() ? (size_t)3 * p3_ring_slot<N, W>() : (size_t)3 * Mx * W;
   return sizeof(V2<T>) * ((size_t)2 * skew8_slots(N, W) + N * W + tw_slots_even<N>() + f);
 }
 template <typename T, int N, int W, bool PF> constexpr size_t axis_smem() {
