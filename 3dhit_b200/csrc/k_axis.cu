@@ -23,6 +23,32 @@
 
 namespace hit {
 
+// Position of a persistent block's tile in the decomposition
+// tile = (c * no + o) * nzt + zt, advanced by the grid stride with carries
+// (the stride is decomposed once) instead of dividing every tile index.
+struct TileWalk {
+  int zt, o, c, dz, dq, dc, nzt, no;
+  __device__ __forceinline__ TileWalk(int t, int stride, int nzt_, int no_) : nzt(nzt_), no(no_) {
+    zt = t % nzt;
+    o = (t / nzt) % no;
+    c = (t / nzt) / no;
+    dz = stride % nzt;
+    dq = (stride / nzt) % no;
+    dc = (stride / nzt) / no;
+  }
+  __device__ __forceinline__ TileWalk next() const {
+    TileWalk w = *this;
+    w.zt += dz;
+    int cy = w.zt >= nzt;
+    if (cy) w.zt -= nzt;
+    w.o += dq + cy;
+    cy = w.o >= no;
+    if (cy) w.o -= no;
+    w.c += dc + cy;
+    return w;
+  }
+};
+
 // PF: the next tile's stored rows are staged in shared memory with cp.async
 // while the current tile is transformed (needs 16-byte aligned rows/columns
 // and whole tiles).  The staging buffer holds all N positions: rows that are
@@ -38,13 +64,8 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
   V2<T>* stg = tws + ((tw_size<false>(N) + 1) / 2 * 2);  // PF: N x W staged rows
   fill_stage_twiddles<T, N, false, NT>(tws, a.tw);
   constexpr int VPC = 16 / sizeof(V2<T>);
-  auto tile_src = [&](int tile) {
-    const int zt = tile % nzt, rest = tile / nzt;
-    const long long o = rest % no, c = rest / no;
-    return a.src + c * a.s_c + o * a.s_o + zt * W;
-  };
-  auto prefetch = [&](int tile) {
-    const V2<T>* src = tile_src(tile);
+  auto prefetch = [&](const TileWalk& w) {
+    const V2<T>* src = a.src + w.c * a.s_c + w.o * a.s_o + w.zt * W;
     constexpr int CPR = W / VPC;  // 16-byte chunks per row
     for (int e = threadIdx.x; e < a.Min * CPR; e += NT) {
       const int row = e / CPR, ch = e % CPR;
@@ -54,13 +75,13 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
   };
   if (PF) {
     for (int e = threadIdx.x; e < (N - a.Min) * W; e += NT) stg[a.hin * W + e] = czero<T>();
-    if (blockIdx.x < ntiles) prefetch(blockIdx.x);
   }
+  TileWalk walk(blockIdx.x, gridDim.x, nzt, no);
+  if (PF && blockIdx.x < ntiles) prefetch(walk);
   __syncthreads();
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int zt = tile % nzt, rest = tile / nzt;
-    const int z0 = zt * W;
-    const long long o = rest % no, c = rest / no;
+    const int z0 = walk.zt * W;
+    const long long o = walk.o, c = walk.c;
     const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
     V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
     const bool zc = PF || z0 + W <= a.nz;  // whole tile inside the valid columns
@@ -69,6 +90,7 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
       __syncthreads();
     }
     const int nxt = tile + gridDim.x;
+    const TileWalk nwalk = walk.next();
     fft_io<T, N, W, NT, TileAddr<N, W>, INV>(
         A, B, tws,
         [&](int pos, int col) {
@@ -81,9 +103,10 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
           if (row >= 0 && (zc || z0 + col < a.nz)) dst[(long long)row * a.d_a + col] = v;
         },
         [&]() {
-          if (PF && nxt < ntiles) prefetch(nxt);
+          if (PF && nxt < ntiles) prefetch(nwalk);
         });
     __syncthreads();  // the next tile's first stage rewrites A
+    walk = nwalk;
   }
   if (PF) cp_async_wait_all();
 }
