@@ -86,9 +86,10 @@ __device__ __forceinline__ float k2_of(float kx, float ky, float kz) {
 __device__ __forceinline__ double k2_of(double kx, double ky, double kz) {
   return __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
 }
-// 1/|k|^2 with 0 at k=0, correctly rounded (grid.py:110-111).
-__device__ __forceinline__ float inv_k2_of(float k2) { return k2 == 0.f ? 0.f : __fdiv_rn(1.f, k2); }
-__device__ __forceinline__ double inv_k2_of(double k2) { return k2 == 0.0 ? 0.0 : __ddiv_rn(1.0, k2); }
+// 1/|k|^2 with 0 at k=0, correctly rounded (grid.py:110-111): the IEEE
+// round-to-nearest reciprocal equals the correctly rounded quotient 1/k2.
+__device__ __forceinline__ float inv_k2_of(float k2) { return k2 == 0.f ? 0.f : __frcp_rn(k2); }
+__device__ __forceinline__ double inv_k2_of(double k2) { return k2 == 0.0 ? 0.0 : __drcp_rn(k2); }
 
 // Wavenumber tables (device): kx[Nx], ky[Ny], kz[Nzh], each value computed on the
 // host as (T)(2*pi/L * n) in double, matching grid.py:101-107.
@@ -97,6 +98,34 @@ template <typename T> struct KTab {
   const T* ky;
   const T* kz;
 };
+
+// Block-wide float64 sums of three values at once (all threads must call;
+// blockDim.x a multiple of 32, scratch >= 96 doubles); valid in thread 0.
+__device__ __forceinline__ void block_sum3_f64(double& a, double& b, double& c, double* scratch) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    scratch[warp] = a;
+    scratch[32 + warp] = b;
+    scratch[64 + warp] = c;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    a = lane < nw ? scratch[lane] : 0.0;
+    b = lane < nw ? scratch[32 + lane] : 0.0;
+    c = lane < nw ? scratch[64 + lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+  }
+}
 
 // Block-wide float64 sum (all threads must call; blockDim.x a multiple of 32).
 __device__ __forceinline__ double block_sum_f64(double v, double* scratch /*>= 32*/) {

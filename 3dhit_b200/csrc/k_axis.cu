@@ -228,12 +228,12 @@ __device__ __forceinline__ void p3_load(const P3Args<T>& a, long long o, V2<T> (
 // (integrators.py:32-38); ns receives the new stage input (or new state) and
 // the float64 partial sums are accumulated.
 template <typename T>
-__device__ __forceinline__ void p3_point(const P3Args<T>& a, int pos, int fy, int z, T ky, T cf, long long o,
+__device__ __forceinline__ void p3_point(const P3Args<T>& a, int pos, int fy, int z, T ky, T kz, T cf, long long o,
                                          V2<T> (&du)[3], const V2<T> (&us)[3], const V2<T> (&ac)[3],
                                          const V2<T> (&uu)[3], V2<T> (&ns)[3], double& sE, double& sO,
                                          double& sB) {
   const Geom& g = a.g;
-  const T kx = a.k.kx[pos], kz = a.k.kz[z];
+  const T kx = __ldg(a.k.kx + pos);
   const T k2 = k2_of(kx, ky, kz);
   const T ik2 = inv_k2_of(k2);
   if (a.forcing == 1) {
@@ -248,7 +248,8 @@ __device__ __forceinline__ void p3_point(const P3Args<T>& a, int pos, int fy, in
 #pragma unroll
     for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], cf));
   }
-  if (!in_dealias(g, pos, fy, z)) {
+  // every stored mode of the dealiased path lies inside the 2/3 box
+  if (g.pruned ? (pos | fy | z) == 0 : !in_dealias(g, pos, fy, z)) {
     du[0] = du[1] = du[2] = czero<T>();
   }
   // projection: div = (kx d0 + ky d1 + kz d2) / k^2 ; d -= k div
@@ -419,6 +420,7 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     const int col = threadIdx.x % W, b = threadIdx.x / W;
     const int z = z0 + col;
     const bool zok = z < g.Mz;
+    const T kz = zok ? __ldg(a.k.kz + z) : T(0);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       // pass r's copies are done (only pass r+1's may be pending) and every
@@ -444,7 +446,7 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
             uu[c] = slot[(6 + c) * (N / 8) * W];
           }
         }
-        p3_point(a, pos, fy, z, ky, cf, o, du, us, ac, uu, ns, sE, sO, sB);
+        p3_point(a, pos, fy, z, ky, kz, cf, o, du, us, ac, uu, ns, sE, sO, sB);
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) f[c][r] = ns[c];
@@ -471,8 +473,8 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
         V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
         if (ok[h]) {
           V2<T> du[3] = {F[e], F[MW + e], F[2 * MW + e]};
-          p3_point(a, full_pos(i, g.hx, g.Mx, N), fy, z0 + col, ky, cf, idx[h], du, us[h], ac[h], uu[h], ns, sE,
-                   sO, sB);
+          p3_point(a, full_pos(i, g.hx, g.Mx, N), fy, z0 + col, ky, __ldg(a.k.kz + z0 + col), cf, idx[h], du, us[h],
+                   ac[h], uu[h], ns, sE, sO, sB);
         }
         if (a.fuse_p1) {
 #pragma unroll
@@ -482,13 +484,12 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     }
   }
   if (a.partial) {
-    const int b = tile;
-    double r = block_sum_f64(sE, red);
-    if (threadIdx.x == 0) a.partial[3 * b + 0] = r;
-    r = block_sum_f64(sO, red);
-    if (threadIdx.x == 0) a.partial[3 * b + 1] = r;
-    r = block_sum_f64(sB, red);
-    if (threadIdx.x == 0) a.partial[3 * b + 2] = r;
+    block_sum3_f64(sE, sO, sB, red);
+    if (threadIdx.x == 0) {
+      a.partial[3 * tile + 0] = sE;
+      a.partial[3 * tile + 1] = sO;
+      a.partial[3 * tile + 2] = sB;
+    }
   }
   if constexpr (REGS) {
     if (a.fuse_p1)
@@ -509,7 +510,7 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
 template <typename T, int N, int W, int NTH>
 __global__ void __launch_bounds__(NTH) k_p3(P3Args<T> a, int nzt, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[32];
+  __shared__ double red[96];
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
   V2<T>* B = A + skew8_slots(N, W);
   V2<T>* stg = B + skew8_slots(N, W);  // staged N x W column of the next nl component
