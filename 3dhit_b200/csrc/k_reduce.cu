@@ -281,11 +281,34 @@ __device__ __forceinline__ double forcing_coef(int forcing, double E, double Om,
   return 0.0;
 }
 
-__global__ void k_finalize_coef(CoefArgs a) {
-  __shared__ double red[32];
-  const double S0 = kahan_column(a.partial, a.nblocks, 3, 0, red);
-  const double S1 = kahan_column(a.partial, a.nblocks, 3, 1, red);
-  const double S2 = kahan_column(a.partial, a.nblocks, 3, 2, red);
+// One 1024-thread block: thread t Kahan-sums rows t, t + 1024, ... of the
+// three columns in order, issuing the loads of CB rows before adding them (the
+// row chain is latency-bound otherwise), then fixed shuffle trees combine the
+// threads.
+constexpr int COEF_THREADS = 1024;
+__global__ void __launch_bounds__(COEF_THREADS) k_finalize_coef(CoefArgs a) {
+  __shared__ double red[96];
+  constexpr int CB = 4;
+  Kahan k0, k1, k2;
+  for (int b0 = threadIdx.x; b0 < a.nblocks; b0 += CB * COEF_THREADS) {
+    double v[CB][3];
+#pragma unroll
+    for (int i = 0; i < CB; ++i) {
+      const int b = b0 + i * COEF_THREADS;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[i][c] = b < a.nblocks ? a.partial[3 * (long long)b + c] : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < CB; ++i) {
+      if (b0 + i * COEF_THREADS < a.nblocks) {
+        k0.add(v[i][0]);
+        k1.add(v[i][1]);
+        k2.add(v[i][2]);
+      }
+    }
+  }
+  double S0 = k0.s - k0.c, S1 = k1.s - k1.c, S2 = k2.s - k2.c;
+  block_sum3_f64(S0, S1, S2, red);
   if (threadIdx.x == 0) {
     const double E = S0 / (2.0 * a.ntot2), Om = S1 / (2.0 * a.ntot2), twoEb = S2 / a.ntot2;
     a.coef[0] = forcing_coef(a.forcing, E, Om, twoEb, a.nu, a.eps, a.E_target, a.tau, a.tiny, 0.0);
@@ -296,7 +319,7 @@ __global__ void k_finalize_coef(CoefArgs a) {
 }
 
 cudaError_t launch_finalize_coef(const CoefArgs& a, cudaStream_t st) {
-  k_finalize_coef<<<1, NT, 0, st>>>(a);
+  k_finalize_coef<<<1, COEF_THREADS, 0, st>>>(a);
   return cudaGetLastError();
 }
 
