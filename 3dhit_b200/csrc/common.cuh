@@ -99,6 +99,14 @@ template <typename T> struct KTab {
   const T* kz;
 };
 
+// Programmatic dependent launch: a kernel launched with launch_pdl may start
+// while the previous kernel in the stream is still finishing.  It sets up what
+// depends on no earlier kernel (twiddle tables, shared-memory zero fill), then
+// pdl_wait() returns once the previous grid has completed and its writes are
+// visible; pdl_trigger() then lets the next kernel start launching.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // Block-wide float64 sums of three values at once (all threads must call;
 // blockDim.x a multiple of 32, scratch >= 96 doubles); valid in thread 0.
 __device__ __forceinline__ void block_sum3_f64(double& a, double& b, double& c, double* scratch) {

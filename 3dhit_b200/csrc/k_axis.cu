@@ -77,6 +77,8 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
     for (int e = threadIdx.x; e < (N - a.Min) * W; e += NT) stg[a.hin * W + e] = czero<T>();
   }
   TileWalk walk(blockIdx.x, gridDim.x, nzt, no);
+  pdl_wait();
+  pdl_trigger();
   if (PF && blockIdx.x < ntiles) prefetch(walk);
   __syncthreads();
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -173,6 +175,8 @@ __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
     const int c = e / ((N - g.Mx) * W), r = e % ((N - g.Mx) * W);
     S[c * NW + g.hx * W + r] = czero<T>();
   }
+  pdl_wait();
+  pdl_trigger();
   const int MW = g.Mx * W;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int j = tile / nzt, z0 = (tile % nzt) * W;
@@ -517,6 +521,8 @@ __global__ void __launch_bounds__(NTH) k_p3(P3Args<T> a, int nzt, int ntiles) {
   V2<T>* tws = stg + N * W;
   V2<T>* F = tws + (tw_size<false>(N) + 1) / 2 * 2;  // 3 x Mx x W, or the register mode's ring
   fill_stage_twiddles<T, N, false, NTH>(tws, a.tw);
+  pdl_wait();
+  pdl_trigger();
   if (blockIdx.x < ntiles) {
     const int jj = blockIdx.x / nzt, zz = (blockIdx.x % nzt) * W;
     const V2<T>* src = a.t3 + (long long)jj * a.g.Mzp + zz;
@@ -584,11 +590,10 @@ cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, 
     if (pf) {
       const size_t smem = axis_smem<T, NN, W, true>();
       if (inv)
-        k_axis<T, NN, W, true, true><<<resident_grid(k_axis<T, NN, W, true, true>, NT, smem, ntiles, c[0]), NT,
-                                       smem, st>>>(a, nzt, no, (int)ntiles);
-      else
-        k_axis<T, NN, W, false, true><<<resident_grid(k_axis<T, NN, W, false, true>, NT, smem, ntiles, c[1]), NT,
-                                        smem, st>>>(a, nzt, no, (int)ntiles);
+        return launch_pdl(k_axis<T, NN, W, true, true>, resident_grid(k_axis<T, NN, W, true, true>, NT, smem, ntiles, c[0]),
+                          NT, smem, st, a, nzt, no, (int)ntiles);
+      return launch_pdl(k_axis<T, NN, W, false, true>, resident_grid(k_axis<T, NN, W, false, true>, NT, smem, ntiles, c[1]),
+                        NT, smem, st, a, nzt, no, (int)ntiles);
     } else {
       const size_t smem = axis_smem<T, NN, W, false>();
       if (inv)
@@ -632,9 +637,8 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p1_v(const P1Ar
   }
   const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
   const size_t smem = p1_smem<T, NN>(W);
-  k_p1<T, NN, W, NTH><<<resident_grid(k_p1<T, NN, W, NTH>, NTH, smem, ntiles, cache), NTH, smem, st>>>(a, nzt,
-                                                                                                        ntiles);
-  return cudaGetLastError();
+  return launch_pdl(k_p1<T, NN, W, NTH>, resident_grid(k_p1<T, NN, W, NTH>, NTH, smem, ntiles, cache), NTH, smem, st, a,
+                    nzt, ntiles);
 }
 
 template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Args<T>& a, cudaStream_t st) {
@@ -647,9 +651,8 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Ar
   }
   const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
   const size_t smem = p3_smem<T, NN, W, NTH>(a.g.Mx);
-  k_p3<T, NN, W, NTH><<<resident_grid(k_p3<T, NN, W, NTH>, NTH, p3_smem<T, NN, W, NTH>(NN), ntiles, cache), NTH,
-                        smem, st>>>(a, nzt, ntiles);
-  return cudaGetLastError();
+  return launch_pdl(k_p3<T, NN, W, NTH>, resident_grid(k_p3<T, NN, W, NTH>, NTH, p3_smem<T, NN, W, NTH>(NN), ntiles, cache),
+                    NTH, smem, st, a, nzt, ntiles);
 }
 
 template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st) {

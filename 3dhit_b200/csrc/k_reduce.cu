@@ -288,6 +288,8 @@ __device__ __forceinline__ double forcing_coef(int forcing, double E, double Om,
 constexpr int COEF_THREADS = 1024;
 __global__ void __launch_bounds__(COEF_THREADS) k_finalize_coef(CoefArgs a) {
   __shared__ double red[96];
+  pdl_wait();
+  pdl_trigger();
   constexpr int CB = 4;
   Kahan k0, k1, k2;
   for (int b0 = threadIdx.x; b0 < a.nblocks; b0 += CB * COEF_THREADS) {
@@ -319,8 +321,7 @@ __global__ void __launch_bounds__(COEF_THREADS) k_finalize_coef(CoefArgs a) {
 }
 
 cudaError_t launch_finalize_coef(const CoefArgs& a, cudaStream_t st) {
-  k_finalize_coef<<<1, COEF_THREADS, 0, st>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_finalize_coef, 1, COEF_THREADS, 0, st, a);
 }
 
 __global__ void k_finalize_sums(SumArgs a) {

@@ -116,6 +116,8 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
     cp_async_commit();
   };
 
+  pdl_wait();
+  pdl_trigger();
   int grp = blockIdx.x;
   if (grp < ngroups) prefetch(grp);
   for (; grp < ngroups; grp += gridDim.x) {
@@ -261,8 +263,7 @@ template <typename T, int HH, int RB, int NTZ, int MINB> cudaError_t launch_zcro
     ready = true;
   }
   const int nb = resident_grid(k_zcross<T, HH, RB, NTZ, MINB>, NTZ, smem, (a.nrows + RB - 1) / RB, cache);
-  k_zcross<T, HH, RB, NTZ, MINB><<<nb, NTZ, smem, st>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_zcross<T, HH, RB, NTZ, MINB>, nb, NTZ, smem, st, a);
 }
 
 template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, cudaStream_t st) {
