@@ -562,3 +562,148 @@ def cfl_dt(u_hat, grid, cfl=0.5):
     umax = float(np.max(np.abs(u[0]) + np.abs(u[1]) + np.abs(u[2])))
     dx = min(grid.Lx / grid.Nx, grid.Ly / grid.Ny, grid.Lz / grid.Nz)
     return cfl * dx / umax
+
+
+# ---------------------------------------------------------------------------
+# Discrete adjoint (no reference counterpart: the reference differentiates
+# through jax.vjp of src/hit3d/navierstokes.py:62-97 and
+# src/hit3d/integrators.py:32-53).  A cotangent is dL/dRe + i dL/dIm of the
+# stored half-spectrum entries, i.e. the inner product is
+# <a, b> = sum Re(conj(a) b) over the stored array; the transpose of a
+# complex-linear operator is then its conjugate transpose.  jax.vjp returns
+# the complex conjugate of these cotangents.
+# ---------------------------------------------------------------------------
+
+
+def _cross(a, b):
+    return np.stack((a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]))
+
+
+def _curl_hat(u_hat, grid):
+    """1j k x u_hat (navierstokes.py:73-77); its own transpose."""
+    kx, ky, kz = grid.kx, grid.ky, grid.kz
+    return 1j * np.stack((ky * u_hat[2] - kz * u_hat[1], kz * u_hat[0] - kx * u_hat[2], kx * u_hat[1] - ky * u_hat[0]))
+
+
+def _dot_re(a, b, extra=None):
+    """sum Re(conj(a) b) in float64 (optionally weighted per mode)."""
+    p = np.real(np.conj(a.astype(np.complex128)) * b.astype(np.complex128))
+    if extra is not None:
+        p = p * extra
+    return float(np.sum(p))
+
+
+def to_physical_T(v, grid):
+    """Transpose of to_physical: w rfftn(v) / N^3 (w = Hermitian weights)."""
+    n3 = grid.Nx * grid.Ny * grid.Nz
+    return (grid.weights * to_spectral(v, grid) / n3).astype(grid.cdtype)
+
+
+def to_spectral_T(v_hat, grid):
+    """Transpose of to_spectral: N^3 irfftn(v_hat / w)."""
+    n3 = grid.Nx * grid.Ny * grid.Nz
+    return (n3 * to_physical(v_hat / grid.weights, grid)).astype(grid.dtype)
+
+
+def forcing_vjp(forcing, u_hat, grid, pv):
+    """Transpose of the derivative of ``forcing.term`` at u_hat applied to pv:
+    (u_hat cotangent, {parameter: cotangent}) (forcing.py:94-95, 138-143 and
+    the hold-energy coefficient)."""
+    ntot2 = float(grid.Nx * grid.Ny * grid.Nz) ** 2
+    w = grid.weights.astype(np.float64)
+    if isinstance(forcing, LinearForcing):
+        return forcing.A * pv, {"A": _dot_re(pv, u_hat)}
+    if isinstance(forcing, BandForcing):
+        mask = forcing._mask(grid)
+        twoE = float(_weighted_2E(u_hat, grid, mask))
+        if not twoE > float(np.finfo(grid.dtype).eps):
+            return np.zeros_like(pv), {"eps": 0.0}
+        c = forcing.eps / twoE
+        beta = _dot_re(pv, u_hat, mask)
+        # c = eps / 2E_band,  d(2E_band)/du = 2 w mask u / Ntot^2
+        ub = c * mask * pv + (beta * (-c / twoE) * 2.0 / ntot2) * (w * mask * u_hat)
+        return ub.astype(grid.cdtype), {"eps": beta / twoE}
+    if isinstance(forcing, HoldEnergyForcing):
+        E, Om = _energy_enstrophy_f64(u_hat, grid)
+        if not E > 0:
+            return np.zeros_like(pv), {"nu": 0.0}
+        A = forcing.coefficient(u_hat, grid)
+        itau = 0.0 if not np.isfinite(forcing.tau) else 1.0 / forcing.tau
+        beta = _dot_re(pv, u_hat)
+        dA_dE = -itau / (2.0 * E) - A / E
+        dA_dO = forcing.nu / E
+        k2 = grid.k2.astype(np.float64)
+        ub = A * pv + (beta / ntot2) * (dA_dE * w + dA_dO * w * k2) * u_hat
+        return ub.astype(grid.cdtype), {"nu": beta * Om / E}
+    return np.zeros_like(pv), {}
+
+
+def rhs_vjp(grid, u_hat, params, v):
+    """Transpose of the RHS derivative at u_hat applied to the cotangent v of
+    rhs(u_hat): returns (u_hat cotangent, {"nu", "A", "eps": cotangents}).
+
+    With g = irfftn(pv / w), pv = project(dealias(v)), u = irfftn(u_hat) and
+    w_ = irfftn(1j k x u_hat), the nonlinear term contributes
+    w (rfftn(w_ x g) + 1j k x rfftn(g x u)); the viscous term -nu k2 v; the
+    forcing term forcing_vjp(pv)."""
+    u_hat = np.asarray(u_hat, grid.cdtype)
+    v = np.asarray(v, grid.cdtype)
+    pv = project(dealias(v, grid), grid)
+    pbar = {"nu": -_dot_re(v, u_hat, grid.k2.astype(np.float64)), "A": 0.0, "eps": 0.0}
+    fb, fp = forcing_vjp(params.forcing, u_hat, grid, pv)
+    for k, val in fp.items():
+        pbar[k] += val
+    u = to_physical(u_hat, grid)
+    om = to_physical(_curl_hat(u_hat, grid), grid)
+    g = to_physical(pv / grid.weights, grid)
+    nl_bar = grid.weights * (to_spectral(_cross(om, g), grid) + _curl_hat(to_spectral(_cross(g, u), grid), grid))
+    ub = nl_bar.astype(grid.cdtype) - params.nu * grid.k2 * v + fb
+    return ub.astype(grid.cdtype), pbar
+
+
+def _add_params(a, b):
+    return {k: a.get(k, 0.0) + b.get(k, 0.0) for k in set(a) | set(b)}
+
+
+def rk4_step_vjp(grid, u_hat, params, dt, ub, t=0.0):
+    """Transpose of rk4_step (integrators.py:32-38) at u_hat applied to the
+    cotangent ub of the new state; the stage inputs are recomputed."""
+    rhs = make_ns_rhs(grid)
+    u_hat = np.asarray(u_hat, grid.cdtype)
+    ub = np.asarray(ub, grid.cdtype)
+    k1 = rhs(u_hat, params, t)
+    s2 = u_hat + 0.5 * dt * k1
+    k2 = rhs(s2, params, t + 0.5 * dt)
+    s3 = u_hat + 0.5 * dt * k2
+    k3 = rhs(s3, params, t + 0.5 * dt)
+    s4 = u_hat + dt * k3
+    sb4, p4 = rhs_vjp(grid, s4, params, (dt / 6.0) * ub)
+    sb3, p3 = rhs_vjp(grid, s3, params, (dt / 3.0) * ub + dt * sb4)
+    sb2, p2 = rhs_vjp(grid, s2, params, (dt / 3.0) * ub + 0.5 * dt * sb3)
+    sb1, p1 = rhs_vjp(grid, u_hat, params, (dt / 6.0) * ub + 0.5 * dt * sb2)
+    pbar = _add_params(_add_params(p1, p2), _add_params(p3, p4))
+    return (ub + sb1 + sb2 + sb3 + sb4).astype(grid.cdtype), pbar
+
+
+def rollout_vjp(grid, u0, params, dt, nsteps, ub, t0=0.0, checkpoint_every=None):
+    """Transpose of rollout (integrators.py:41-53): states are kept every
+    ``checkpoint_every`` steps and recomputed segment by segment."""
+    K = nsteps if not checkpoint_every else int(checkpoint_every)
+    rhs = make_ns_rhs(grid)
+    ckpt = []
+    u = np.asarray(u0, grid.cdtype)
+    for i in range(nsteps):
+        if i % K == 0:
+            ckpt.append(u)
+        u = rk4_step(rhs, u, params, dt, t0 + i * dt)
+    ub = np.asarray(ub, grid.cdtype)
+    pbar = {"nu": 0.0, "A": 0.0, "eps": 0.0}
+    for j in range(len(ckpt) - 1, -1, -1):
+        i0 = j * K
+        seg = [ckpt[j]]
+        for i in range(i0, min(i0 + K, nsteps) - 1):
+            seg.append(rk4_step(rhs, seg[-1], params, dt, t0 + i * dt))
+        for i in range(len(seg) - 1, -1, -1):
+            ub, p = rk4_step_vjp(grid, seg[i], params, dt, ub, t0 + (i0 + i) * dt)
+            pbar = _add_params(pbar, p)
+    return ub, pbar
