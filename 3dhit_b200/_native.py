@@ -70,6 +70,9 @@ SIGNATURES = {
     "hit_rk4_step": (_i, [_vp, _vp, _PP, _d, _d, _vp, _vp]),
     "hit_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _d, _vp, _vp]),
     "hit_profile_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _vp, _vp, _vp, _vp]),
+    "hit_rhs_vjp": (_i, [_vp, _vp, _PP, _d, _vp, _vp, _vp, _vp]),
+    "hit_rk4_step_vjp": (_i, [_vp, _vp, _PP, _d, _d, _vp, _vp, _vp, _vp]),
+    "hit_rollout_vjp": (_i, [_vp, _vp, _PP, _d, _i64, _d, _i, _vp, _vp, _vp, _vp]),
     "hit_energy_spectrum": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "hit_energy_budget": (_i, [_vp, _vp, _PP, _vp, _vp]),
     "hit_energy_spectrum_noalloc": (_i, [_i, _i, _i, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),

@@ -176,6 +176,34 @@ struct CoefArgs {
 };
 cudaError_t launch_finalize_coef(const CoefArgs& a, cudaStream_t st);
 
+// Discrete adjoint of the RHS (k_adjoint.cu), reference layout.
+template <typename T> struct AdjArgs {
+  const V2<T>* u;   // state (3, Nx, Ny, Nzh)
+  const V2<T>* v;   // cotangent of rhs(u)
+  V2<T>* x9;        // transform inputs [u, 1j k x u, pv / w] (9 components)
+  const V2<T>* s6;  // rfftn(om x g), rfftn(g x u) (6 components)
+  V2<T>* ub;        // cotangent of u (output)
+  const double* scal;
+  double* partial;  // 6 per block
+  Geom g;
+  KTab<T> k;
+  T nu, kmin2, kmax2;
+};
+struct AdjCoefArgs {
+  const double* sums;  // the 6 finalised sums
+  double* scal;        // 5 scalars for k_adj_prep
+  double* pct;         // parameter cotangents (nu, A, eps), added to
+  int forcing;
+  double ntot2, nu, A, eps, E_target, tau, tiny;
+};
+template <typename T> cudaError_t launch_adj_sums(const AdjArgs<T>& a, int nblocks, cudaStream_t st);
+cudaError_t launch_adj_coef(const AdjCoefArgs& a, cudaStream_t st);
+template <typename T> cudaError_t launch_adj_prep(const AdjArgs<T>& a, cudaStream_t st);
+template <typename T> cudaError_t launch_adj_cross(T* p, long long n, cudaStream_t st);
+template <typename T> cudaError_t launch_adj_combine(const AdjArgs<T>& a, cudaStream_t st);
+template <typename T>
+cudaError_t launch_axpby(const V2<T>* x, T alpha, const V2<T>* y, T beta, V2<T>* out, long long n, cudaStream_t st);
+
 struct SumArgs {
   const double* partial;
   int nblocks, nvals;

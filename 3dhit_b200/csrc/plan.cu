@@ -138,6 +138,10 @@ struct hit_plan {
   Buf xws;                // to_physical / to_spectral workspace
   Buf dpartial, dsums;    // diagnostics partials / sums
   int diag_blocks = 0;
+  // adjoint workspace (reference layout): transform inputs/outputs of the RHS
+  // transpose, its float64 sums and scalars, the RK4 stage inputs and
+  // cotangents, and the rollout checkpoints
+  Buf ax9, aph, as6, apart, asums, ascal, apct, ast[3], ak, akb, asb, aacc, aub, ack, aseg;
   cudaStream_t cap = nullptr;  // private stream used only for graph capture
 };
 
@@ -621,6 +625,173 @@ int diag_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double* E, d
   return HIT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// discrete adjoint (general path, reference layout): RHS transpose, RK4 step
+// transpose (stage inputs recomputed), rollout transpose with checkpoints
+// ---------------------------------------------------------------------------
+
+template <typename T> int adj_blocks(const hit_plan* p) {
+  const long long nm = (long long)p->Nx * p->Ny * (p->Nz / 2 + 1);
+  return (int)std::min<long long>((nm + NT - 1) / NT, 8 * 148);
+}
+
+// ub = (d rhs / d u)^T v at u; the parameter cotangents (nu, A, eps) are added
+// to pct (device).
+template <typename T>
+int rhs_vjp_impl(hit_plan* p, const V2<T>* u, const Scalars& s, const V2<T>* v, V2<T>* ub, double* pct,
+                 cudaStream_t st) {
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  const long long nm = (long long)g.Nx * g.Ny * g.Nzh, n3 = (long long)g.Nx * g.Ny * g.Nz;
+  const int nb = adj_blocks<T>(p);
+  int rc;
+  if ((rc = ensure(p->ax9, 9 * nm * sizeof(V2<T>)))) return rc;
+  if ((rc = ensure(p->aph, 9 * n3 * sizeof(T)))) return rc;
+  if ((rc = ensure(p->as6, 6 * nm * sizeof(V2<T>)))) return rc;
+  if ((rc = ensure(p->apart, (size_t)nb * 6 * sizeof(double)))) return rc;
+  if ((rc = ensure(p->asums, 6 * sizeof(double)))) return rc;
+  if ((rc = ensure(p->ascal, 8 * sizeof(double)))) return rc;
+  AdjArgs<T> a{};
+  a.u = u;
+  a.v = v;
+  a.x9 = vp<T>(p->ax9);
+  a.s6 = vp<T>(p->as6);
+  a.ub = ub;
+  a.scal = static_cast<const double*>(p->ascal.p);
+  a.partial = static_cast<double*>(p->apart.p);
+  a.g = g;
+  a.k = ktab_of<T>(p);
+  a.nu = (T)s.nu;
+  a.kmin2 = (T)s.kmin2;
+  a.kmax2 = (T)s.kmax2;
+  HIT_CK(launch_adj_sums<T>(a, nb, st));
+  SumArgs sa{static_cast<const double*>(p->apart.p), nb, 6, static_cast<double*>(p->asums.p)};
+  HIT_CK(launch_finalize_sums(sa, st));
+  AdjCoefArgs c{};
+  c.sums = static_cast<const double*>(p->asums.p);
+  c.scal = static_cast<double*>(p->ascal.p);
+  c.pct = pct;
+  c.forcing = s.forcing;
+  c.ntot2 = ntot2_of(p);
+  c.nu = s.nu;
+  c.A = s.A;
+  c.eps = s.eps;
+  c.E_target = s.E_target;
+  c.tau = s.tau;
+  c.tiny = tiny_of<T>();
+  HIT_CK(launch_adj_coef(c, st));
+  HIT_CK(launch_adj_prep<T>(a, st));
+  if ((rc = to_physical_impl<T>(p, p->ax9.p, 9, p->aph.p, st))) return rc;
+  HIT_CK(launch_adj_cross<T>(static_cast<T*>(p->aph.p), n3, st));
+  if ((rc = to_spectral_impl<T>(p, static_cast<T*>(p->aph.p) + 3 * n3, 6, p->as6.p, st))) return rc;
+  HIT_CK(launch_adj_combine<T>(a, st));
+  return HIT_OK;
+}
+
+hit_params general_params(const hit_params* pr) {
+  hit_params q = *pr;
+  q.flags &= ~(unsigned)HIT_FLAG_ASSUME_DEALIASED;  // recompute on the general path
+  return q;
+}
+
+// ub_out = (d rk4_step / d u)^T ub_in at u (stage inputs recomputed); ub_out
+// may alias ub_in.
+template <typename T>
+int rk4_vjp_impl(hit_plan* p, const V2<T>* u, const hit_params* pr, double dt, const V2<T>* ub_in, V2<T>* ub_out,
+                 double* pct, cudaStream_t st) {
+  const long long n = 3LL * p->Nx * p->Ny * (p->Nz / 2 + 1);
+  const size_t bytes = n * sizeof(V2<T>);
+  int rc;
+  for (Buf* b : {&p->ast[0], &p->ast[1], &p->ast[2], &p->ak, &p->akb, &p->asb, &p->aacc})
+    if ((rc = ensure(*b, bytes))) return rc;
+  const hit_params pg = general_params(pr);
+  const Scalars s = scalars_of(pr);
+  V2<T>* S2 = vp<T>(p->ast[0]);
+  V2<T>* S3 = vp<T>(p->ast[1]);
+  V2<T>* S4 = vp<T>(p->ast[2]);
+  V2<T>* K = vp<T>(p->ak);
+  V2<T>* KB = vp<T>(p->akb);
+  V2<T>* SB = vp<T>(p->asb);
+  V2<T>* ACC = vp<T>(p->aacc);
+  const T h = (T)(0.5 * dt), d = (T)dt, d3 = (T)(dt / 3.0), d6 = (T)(dt / 6.0);
+  // stage inputs (integrators.py:32-38)
+  if ((rc = rhs_impl<T>(p, u, &pg, K, st))) return rc;
+  HIT_CK(launch_axpby<T>(u, T(1), K, h, S2, n, st));
+  if ((rc = rhs_impl<T>(p, S2, &pg, K, st))) return rc;
+  HIT_CK(launch_axpby<T>(u, T(1), K, h, S3, n, st));
+  if ((rc = rhs_impl<T>(p, S3, &pg, K, st))) return rc;
+  HIT_CK(launch_axpby<T>(u, T(1), K, d, S4, n, st));
+  // transpose of u + dt/6 (k1 + 2 k2 + 2 k3 + k4), stage by stage backwards
+  HIT_CK(launch_axpby<T>(ub_in, d6, nullptr, T(0), KB, n, st));
+  if ((rc = rhs_vjp_impl<T>(p, S4, s, KB, SB, pct, st))) return rc;
+  HIT_CK(launch_axpby<T>(ub_in, T(1), SB, T(1), ACC, n, st));
+  HIT_CK(launch_axpby<T>(ub_in, d3, SB, d, KB, n, st));
+  if ((rc = rhs_vjp_impl<T>(p, S3, s, KB, SB, pct, st))) return rc;
+  HIT_CK(launch_axpby<T>(ACC, T(1), SB, T(1), ACC, n, st));
+  HIT_CK(launch_axpby<T>(ub_in, d3, SB, h, KB, n, st));
+  if ((rc = rhs_vjp_impl<T>(p, S2, s, KB, SB, pct, st))) return rc;
+  HIT_CK(launch_axpby<T>(ACC, T(1), SB, T(1), ACC, n, st));
+  HIT_CK(launch_axpby<T>(ub_in, d6, SB, h, KB, n, st));
+  if ((rc = rhs_vjp_impl<T>(p, u, s, KB, SB, pct, st))) return rc;
+  HIT_CK(launch_axpby<T>(ACC, T(1), SB, T(1), ub_out, n, st));
+  return HIT_OK;
+}
+
+// u0_bar = (d rollout / d u0)^T ub at u0: states every K steps are kept (the
+// forward runs as graph-replayed steps), each segment is recomputed forwards
+// and transposed step by step backwards.
+template <typename T>
+int rollout_vjp_impl(hit_plan* p, const void* u0, const hit_params* pr, double dt, int64_t nsteps, int K,
+                     const void* ub, void* u0_bar, double* pct, cudaStream_t st) {
+  const long long n = 3LL * p->Nx * p->Ny * (p->Nz / 2 + 1);
+  const size_t bytes = n * sizeof(V2<T>);
+  const int64_t nseg = (nsteps + K - 1) / K;
+  int rc;
+  if ((rc = ensure(p->ack, std::max<int64_t>(nseg, 1) * bytes))) return rc;
+  if ((rc = ensure(p->aseg, (size_t)K * bytes))) return rc;
+  if ((rc = ensure(p->aub, bytes))) return rc;
+  const hit_params pg = general_params(pr);
+  V2<T>* CK = vp<T>(p->ack);
+  V2<T>* SEG = vp<T>(p->aseg);
+  V2<T>* UB = vp<T>(p->aub);
+  HIT_CK(cudaMemcpyAsync(UB, ub, bytes, cudaMemcpyDeviceToDevice, st));
+  if (nsteps == 0) {
+    HIT_CK(cudaMemcpyAsync(u0_bar, UB, bytes, cudaMemcpyDeviceToDevice, st));
+    return HIT_OK;
+  }
+  HIT_CK(cudaMemcpyAsync(CK, u0, bytes, cudaMemcpyDeviceToDevice, st));
+  for (int64_t j = 1; j < nseg; ++j)
+    if ((rc = rollout_impl<T>(p, CK + (j - 1) * n, &pg, dt, K, CK + j * n, st))) return rc;
+  for (int64_t j = nseg - 1; j >= 0; --j) {
+    const int len = (int)std::min<int64_t>(K, nsteps - j * K);
+    HIT_CK(cudaMemcpyAsync(SEG, CK + j * n, bytes, cudaMemcpyDeviceToDevice, st));
+    for (int i = 1; i < len; ++i)
+      if ((rc = rollout_impl<T>(p, SEG + (i - 1) * n, &pg, dt, 1, SEG + i * n, st))) return rc;
+    for (int i = len - 1; i >= 0; --i)
+      if ((rc = rk4_vjp_impl<T>(p, SEG + i * n, pr, dt, UB, UB, pct, st))) return rc;
+  }
+  HIT_CK(cudaMemcpyAsync(u0_bar, UB, bytes, cudaMemcpyDeviceToDevice, st));
+  return HIT_OK;
+}
+
+// entry-point wrappers: zero the parameter cotangents, run, copy them out
+template <typename T>
+int vjp_entry(hit_plan* p, int which, const void* u, const hit_params* pr, double dt, int64_t nsteps, int K,
+              const void* ct, void* ubar, double* pct_out, cudaStream_t st) {
+  int rc;
+  if ((rc = ensure(p->apct, 4 * sizeof(double)))) return rc;
+  double* pct = static_cast<double*>(p->apct.p);
+  HIT_CK(cudaMemsetAsync(pct, 0, 4 * sizeof(double), st));
+  const V2<T>* uu = static_cast<const V2<T>*>(u);
+  const V2<T>* cc = static_cast<const V2<T>*>(ct);
+  V2<T>* ub = static_cast<V2<T>*>(ubar);
+  if (which == 0) rc = rhs_vjp_impl<T>(p, uu, scalars_of(pr), cc, ub, pct, st);
+  else if (which == 1) rc = rk4_vjp_impl<T>(p, uu, pr, dt, cc, ub, pct, st);
+  else rc = rollout_vjp_impl<T>(p, u, pr, dt, nsteps, K, ct, ubar, pct, st);
+  if (rc) return rc;
+  if (pct_out) HIT_CK(cudaMemcpyAsync(pct_out, pct, 3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return HIT_OK;
+}
+
 template <typename T> void fill_tables(hit_plan* p, std::string& kt, std::string& tw) {
   const double two_pi = 2.0 * M_PI;
   const int Nzh = p->Nz / 2 + 1;
@@ -731,6 +902,9 @@ int hit_plan_destroy(hit_plan* p) {
   release(p->xws);
   release(p->dpartial);
   release(p->dsums);
+  for (Buf* b : {&p->ax9, &p->aph, &p->as6, &p->apart, &p->asums, &p->ascal, &p->apct, &p->ast[0], &p->ast[1],
+                 &p->ast[2], &p->ak, &p->akb, &p->asb, &p->aacc, &p->aub, &p->ack, &p->aseg})
+    release(*b);
   if (p->cap) cudaStreamDestroy(p->cap);
   delete p;
   return HIT_OK;
@@ -830,6 +1004,39 @@ int hit_profile_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, do
   if ((rc = check_params(pr))) return rc;
   DeviceGuard dg(p->device);
   return DISPATCH(p, profile_impl)(p, u_hat, pr, dt, nsteps, out, ms, launches, (cudaStream_t)stream);
+}
+
+int hit_rhs_vjp(hit_plan* p, const void* u_hat, const hit_params* pr, double t, const void* ct, void* u_bar,
+                double* param_ct, void* stream) {
+  (void)t;
+  if (!p || !u_hat || !ct || !u_bar) return fail(HIT_E_INVALID, "NULL argument");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, vjp_entry)(p, 0, u_hat, pr, 0.0, 0, 1, ct, u_bar, param_ct, (cudaStream_t)stream);
+}
+
+int hit_rk4_step_vjp(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, double t, const void* ct,
+                     void* u_bar, double* param_ct, void* stream) {
+  (void)t;
+  if (!p || !u_hat || !ct || !u_bar) return fail(HIT_E_INVALID, "NULL argument");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, vjp_entry)(p, 1, u_hat, pr, dt, 1, 1, ct, u_bar, param_ct, (cudaStream_t)stream);
+}
+
+int hit_rollout_vjp(hit_plan* p, const void* u0, const hit_params* pr, double dt, int64_t nsteps, double t0,
+                    int checkpoint_every, const void* ct, void* u0_bar, double* param_ct, void* stream) {
+  (void)t0;
+  if (!p || !u0 || !ct || !u0_bar) return fail(HIT_E_INVALID, "NULL argument");
+  if (nsteps < 0) return fail(HIT_E_INVALID, "nsteps must be >= 0");
+  if (checkpoint_every < 1) return fail(HIT_E_INVALID, "checkpoint_every must be >= 1");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  const int K = (int)std::min<int64_t>(checkpoint_every, std::max<int64_t>(nsteps, 1));
+  return DISPATCH(p, vjp_entry)(p, 2, u0, pr, dt, nsteps, K, ct, u0_bar, param_ct, (cudaStream_t)stream);
 }
 
 int hit_energy_spectrum(hit_plan* p, const void* u_hat, double* E, double* Ec, void* stream) {

@@ -118,6 +118,34 @@ int hit_rk4_step(hit_plan *plan, const void *u_hat, const hit_params *params,
 int hit_rollout(hit_plan *plan, const void *u_hat, const hit_params *params,
                 double dt, int64_t nsteps, double t0, void *out, void *stream);
 
+/* Discrete adjoint (vector-Jacobian products).  The reference obtains these
+ * with jax.vjp of rhs / rk4_step / rollout (src/hit3d/navierstokes.py:62-97,
+ * src/hit3d/integrators.py:32-53).  Cotangents are arrays in the state layout
+ * holding dL/dRe + i dL/dIm of the stored entries (PyTorch's convention; a JAX
+ * custom_vjp rule conjugates them on the way in and out).  param_ct_dev, when
+ * not NULL, is a DEVICE double[3] that receives the cotangents of (nu, A, eps)
+ * of `params` (A: linear forcing; eps: band forcing; for the hold-energy
+ * forcing nu also enters its coefficient).  The transposes run on the general
+ * (full-layout) path in the plan's dtype and recompute what they need:
+ *   hit_rhs_vjp       u_bar = (d rhs/d u)^T ct at u_hat;
+ *   hit_rk4_step_vjp  u_bar = (d rk4_step/d u)^T ct (stage inputs recomputed);
+ *   hit_rollout_vjp   u0_bar = (d rollout/d u0)^T ct: states are kept every
+ *                     checkpoint_every steps, each segment is recomputed and
+ *                     transposed step by step (memory: nsteps/checkpoint_every
+ *                     + checkpoint_every states).
+ * u_bar may alias ct. */
+int hit_rhs_vjp(hit_plan *plan, const void *u_hat, const hit_params *params,
+                double t, const void *ct, void *u_bar, double *param_ct_dev,
+                void *stream);
+int hit_rk4_step_vjp(hit_plan *plan, const void *u_hat,
+                     const hit_params *params, double dt, double t,
+                     const void *ct, void *u_bar, double *param_ct_dev,
+                     void *stream);
+int hit_rollout_vjp(hit_plan *plan, const void *u0_hat,
+                    const hit_params *params, double dt, int64_t nsteps,
+                    double t0, int checkpoint_every, const void *ct,
+                    void *u0_bar, double *param_ct_dev, void *stream);
+
 /* Measurement hook (no reference counterpart): the same nsteps RK4 steps as
  * hit_rollout, launched one kernel at a time with a CUDA event pair around
  * every launch on `stream`.  Host arrays ms_out / launches_out of
