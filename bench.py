@@ -193,6 +193,113 @@ def run_reference(args):
     return 0
 
 
+def run_adjoint(args):
+    """Adjoint rollout (decaying HIT, N^3 fp32, k0=4, u_rms=1, nu=4e-3, CFL 0.5):
+    loss = squared log-error of the final E(k) over the energy-containing
+    shells 1..N/8 against a seeded target spectrum (the final spectrum of the
+    same rollout from a second seeded field); gradient w.r.t. the initial state and
+    the Lundgren coefficient A (LinearForcing, A = 0) through the hand-written
+    adjoint with checkpoints every K steps, checked against central finite
+    differences (h = 1e-3) on seeded random directions, in float32 and in
+    float64.  Prints one JSON line: adjoint/forward time ratio, times, device
+    memory, finite-difference errors."""
+    h3 = importlib.import_module("3dhit_b200")
+    dev = torch.device("cuda", 0)
+    N, n, K, ndir, h = args.adj_size, args.adj_steps, args.adj_ckpt, args.adj_dirs, 1e-3
+    nu = 4e-3
+    free0, total = torch.cuda.mem_get_info(dev)
+    res = {}
+    for dtype in (torch.float32, torch.float64):
+        g = h3.make_grid(N, dtype=dtype, device=dev)
+        rhs = h3.make_ns_rhs(g)
+        u0 = h3.hit_initial_field(0, g)
+        dt = h3.cfl_dt(u0, g, CFL)
+        S = N // 8
+        k0 = 2 * np.pi / g.Lx
+        shell = torch.floor(torch.sqrt(g.k2) / k0 + 0.5).to(torch.int64).expand(u0.shape[1:]).reshape(-1)
+        w = g.weights.to(torch.float64).expand(u0.shape[1:]).reshape(-1)
+        sel = ((shell >= 1) & (shell <= S)).to(torch.float64)
+        n2 = float(N) ** 6
+
+        def spec(u):
+            a2 = (u.abs() ** 2).sum(0).reshape(-1).to(torch.float64)
+            return torch.bincount(shell, weights=w * a2, minlength=S + 1)[: S + 1] / (2 * n2)
+
+        def params(A):
+            return h3.NSParams(nu=nu, forcing=h3.LinearForcing(A))
+
+        target = h3.rollout(rhs, h3.hit_initial_field(1, g), params(0.0), dt, n, assume_dealiased=False)
+        logT = torch.log(spec(target)[1:])
+
+        def loss_and_ct(u):
+            E = spec(u)
+            r = torch.log(E[1:]) - logT
+            L = float((r ** 2).sum())
+            coef = torch.zeros(S + 1, dtype=torch.float64, device=dev)
+            coef[1:] = 2 * r / E[1:]
+            c = (coef[shell.clamp(max=S)] * sel * w / n2).reshape(u.shape[1:])
+            return L, (c.to(u.real.dtype) * u).contiguous()
+
+        def L_of(u, A=0.0):
+            return loss_and_ct(h3.rollout(rhs, u, params(A), dt, n, assume_dealiased=False))[0]
+
+        uT = h3.rollout(rhs, u0, params(0.0), dt, n, assume_dealiased=False)  # warm-up (graphs)
+        L0, ct = loss_and_ct(uT)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        h3.rollout(rhs, u0, params(0.0), dt, n, assume_dealiased=False)
+        e1.record()
+        torch.cuda.synchronize()
+        fwd_ms = e0.elapsed_time(e1)
+        h3.rollout_vjp(rhs, u0, params(0.0), dt, 2, ct, checkpoint_every=K)  # warm-up (workspace)
+        torch.cuda.synchronize()
+        e0.record()
+        ub, pb = h3.rollout_vjp(rhs, u0, params(0.0), dt, n, ct, checkpoint_every=K)
+        e1.record()
+        torch.cuda.synchronize()
+        adj_ms = e0.elapsed_time(e1)
+        free1, _ = torch.cuda.mem_get_info(dev)
+        errs = []
+        for i in range(ndir):
+            d = h3.random_field(1000 + i, g)  # seeded solenoidal, dealiased direction
+            d = d * (torch.linalg.vector_norm(u0) / torch.linalg.vector_norm(d))
+            fd = (L_of(u0 + h * d) - L_of(u0 - h * d)) / (2 * h)
+            ad = float(torch.sum(torch.real(torch.conj(ub) * d)))
+            errs.append(abs(ad - fd) / max(abs(fd), 1e-30))
+        fdA = (L_of(u0, h) - L_of(u0, -h)) / (2 * h)
+        conv = None
+        if dtype == torch.float64:  # truncation check: the same directions with h = 1e-5
+            conv = []
+            for i in range(ndir):
+                d = h3.random_field(1000 + i, g)
+                d = d * (torch.linalg.vector_norm(u0) / torch.linalg.vector_norm(d))
+                fd = (L_of(u0 + 1e-5 * d) - L_of(u0 - 1e-5 * d)) / 2e-5
+                ad = float(torch.sum(torch.real(torch.conj(ub) * d)))
+                conv.append(abs(ad - fd) / max(abs(fd), 1e-30))
+        res["f32" if dtype == torch.float32 else "f64"] = {
+            "loss": L0, "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "ratio": adj_ms / fwd_ms,
+            "device_mem_used_gb": (free0 - free1) / 1e9,
+            "fd_rel_err_u0": errs, "fd_rel_err_u0_max": max(errs),
+            "dL_dA": pb["A"], "fd_dL_dA": fdA, "fd_rel_err_A": abs(pb["A"] - fdA) / max(abs(fdA), 1e-30),
+            "dt": dt,
+        }
+        if conv is not None:
+            res["f64"]["fd_h1e-5_rel_err_u0"] = conv
+            res["f64"]["fd_h1e-5_rel_err_u0_max"] = max(conv)
+        del g, rhs
+    line = {"metric": f"adjoint rollout {N}^3 fp32: adjoint/forward time ratio", "value": res["f32"]["ratio"],
+            "unit": "x", "higher_is_better": False, "n_gpus": 1,
+            "config": {"workload": f"decaying HIT {N}^3, k0=4, u_rms=1, nu=4e-3, CFL 0.5, {n} RK4 steps, "
+                                   f"checkpoints every {K}; loss = squared log-error of E(k), shells 1..{N // 8}, "
+                                   f"vs the final spectrum of the same rollout from seed 1; gradient w.r.t. u0 "
+                                   f"and Lundgren A (=0)",
+                       "fd": f"central, h={h}, {ndir} seeded solenoidal directions scaled to |u0|"},
+            "f32": res["f32"], "f64": res["f64"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,9 +312,16 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--adjoint", action="store_true", help="adjoint rollout check instead of the step benchmark")
+    ap.add_argument("--adj-size", type=int, default=128)
+    ap.add_argument("--adj-steps", type=int, default=400)
+    ap.add_argument("--adj-ckpt", type=int, default=20)
+    ap.add_argument("--adj-dirs", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.adjoint:
+        return run_adjoint(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
