@@ -75,6 +75,7 @@ SIGNATURES = {
     "hit_rollout_vjp": (_i, [_vp, _vp, _PP, _d, _i64, _d, _i, _vp, _vp, _vp, _vp]),
     "hit_energy_spectrum": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "hit_energy_budget": (_i, [_vp, _vp, _PP, _vp, _vp]),
+    "hit_tc_gemm_bf16": (_i, [_vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp, _vp]),
     "hit_energy_spectrum_noalloc": (_i, [_i, _i, _i, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "hit_last_error_string": (ctypes.c_char_p, []),
 }

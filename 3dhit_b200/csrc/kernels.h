@@ -7,6 +7,8 @@
 
 #include <utility>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace hit {
@@ -203,6 +205,9 @@ template <typename T> cudaError_t launch_adj_cross(T* p, long long n, cudaStream
 template <typename T> cudaError_t launch_adj_combine(const AdjArgs<T>& a, cudaStream_t st);
 template <typename T>
 cudaError_t launch_axpby(const V2<T>* x, T alpha, const V2<T>* y, T beta, V2<T>* out, long long n, cudaStream_t st);
+
+cudaError_t launch_tcgemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M,
+                          int N, int K, int* err, cudaStream_t st);
 
 struct SumArgs {
   const double* partial;

@@ -1039,6 +1039,19 @@ int hit_rollout_vjp(hit_plan* p, const void* u0, const hit_params* pr, double dt
   return DISPATCH(p, vjp_entry)(p, 2, u0, pr, dt, nsteps, K, ct, u0_bar, param_ct, (cudaStream_t)stream);
 }
 
+int hit_tc_gemm_bf16(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M, int N, int K, int* err,
+                     void* stream) {
+  if (!A || !B || !C || !err) return fail(HIT_E_INVALID, "NULL argument");
+  if (M < 1 || K < 16 || K % 16 || lda % 8 || ldb % 8 || lda < K || ldb < K || ldc < N)
+    return fail(HIT_E_INVALID, "tc_gemm: M >= 1, K a multiple of 16, lda/ldb multiples of 8 and >= K, ldc >= N");
+  if (N != 16 && N != 32 && N != 64 && N != 128) return fail(HIT_E_INVALID, "tc_gemm: N in {16, 32, 64, 128}");
+  if (((uintptr_t)A | (uintptr_t)B) % 16) return fail(HIT_E_INVALID, "tc_gemm: A and B must be 16-byte aligned");
+  cudaError_t e = launch_tcgemm(static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B), ldb, C,
+                                ldc, M, N, K, err, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "tc_gemm");
+  return HIT_OK;
+}
+
 int hit_energy_spectrum(hit_plan* p, const void* u_hat, double* E, double* Ec, void* stream) {
   if (!p || !u_hat) return fail(HIT_E_INVALID, "NULL argument");
   if (!E && !Ec) return fail(HIT_E_INVALID, "no output requested");

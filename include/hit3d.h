@@ -173,6 +173,15 @@ int hit_energy_spectrum(hit_plan *plan, const void *u_hat, double *E_dev,
 int hit_energy_budget(hit_plan *plan, const void *u_hat,
                       const hit_params *params, double *out_dev, void *stream);
 
+/* BF16 GEMM on the fifth-generation tensor cores (no reference counterpart;
+ * the building block of the learned subgrid-stress closure):
+ *   C[M][N] (float32, row-major, ldc) = A[M][K] * B[N][K]^T
+ * with A, B bf16 row-major (lda, ldb in elements, multiples of 8, 16-byte
+ * aligned rows), N in {16, 32, 64, 128}, K a positive multiple of 16.
+ * err_dev (DEVICE int) is set to 1 if a tensor-core wait timed out. */
+int hit_tc_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C,
+                     int ldc, int M, int N, int K, int *err_dev, void *stream);
+
 /* energy_spectrum without any device allocation.  No counterpart in the
  * reference: it serves callers that cannot allocate device memory -- code
  * running while its stream is being captured into a CUDA graph, an XLA custom
