@@ -76,9 +76,17 @@ SIGNATURES = {
     "hit_energy_spectrum": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "hit_energy_budget": (_i, [_vp, _vp, _PP, _vp, _vp]),
     "hit_tc_gemm_bf16": (_i, [_vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp, _vp]),
+    "hit_mlp_forward": (_i, [_vp, _vp, _i64, _vp, _vp, _vp]),
+    "hit_mlp_workspace_bytes": (_i64, [_i64]),
+    "hit_mlp_train_grads": (_i, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hit_energy_spectrum_noalloc": (_i, [_i, _i, _i, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "hit_last_error_string": (ctypes.c_char_p, []),
 }
+
+
+class MlpWeights(ctypes.Structure):
+    """hit_mlp_weights (include/hit3d.h): device pointers of the closure MLP."""
+    _fields_ = [(n, ctypes.c_void_p) for n in ("w1t", "w2t", "w3t", "w4t", "w2", "w3", "w4", "b2", "b3", "b4")]
 
 
 class HitError(RuntimeError):

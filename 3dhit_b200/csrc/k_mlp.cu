@@ -1,0 +1,253 @@
+// Pointwise MLP of the learned subgrid-stress closure on the fifth-generation
+// tensor cores: 9 -> 64 -> 64 -> 64 -> 6, GELU (erf form) between layers, bf16
+// weights and activations, float32 accumulation in TMEM.
+//
+// One persistent CTA of 128 threads works on 128-point tiles; thread t owns
+// point t of the tile (its TMEM lane).  The seven weight operands (the forward
+// W^T of every layer and the backward W of layers 2-4) stay in shared memory
+// in the K-major core-matrix layout (tc_common.cuh).  Per tile:
+//   forward   z1 = [x, 0, 1] W1 (bias in row 15), a_l = gelu(z_l),
+//             z_l = a_{l-1} W_l + b_l (l = 2, 3), y = a3 W4 + b4;
+//   training  dy = 2 (y - tau) / (P * 6) (the MSE loss), then
+//             da_{l-1} = dz_l W_l^T, dz_{l-1} = da_{l-1} * gelu'(z_{l-1}),
+// the pre-activations z1..z3 staying in TMEM for gelu'.  The activations
+// a_{l-1} (with a ones row for the bias) and the dz_l are written feature-major
+// (aT[f][p], dzT[f][p], bf16) for the weight-gradient GEMMs
+// dW_l = a_{l-1}^T dz_l, which run on the same tensor cores (k_tcgemm).
+#include <cuda_bf16.h>
+
+#include "kernels.h"
+#include "tc_common.cuh"
+
+namespace hit {
+
+namespace {
+constexpr int MLP_WAIT = 1 << 22;
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float x) {
+  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// Copy a row-major bf16 matrix [R][KC] into the K-major core-matrix layout.
+__device__ __forceinline__ void load_kmajor(unsigned char* dst, const __nv_bfloat16* __restrict__ src, int R, int KC) {
+  for (int e = threadIdx.x; e < R * (KC / 8); e += blockDim.x) {
+    const int r = e / (KC / 8), c8 = e % (KC / 8);
+    *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, c8 * 8, KC)) =
+        *reinterpret_cast<const uint4*>(src + (long long)r * KC + c8 * 8);
+  }
+}
+
+// This thread's row (point) of a K-major tile with KC columns from n floats
+// (columns past n are zero).
+template <int KC>
+__device__ __forceinline__ void store_row(unsigned char* tile, int row, const float* v, int n) {
+#pragma unroll
+  for (int c8 = 0; c8 < KC / 8; ++c8) {
+    __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16_rn(c8 * 8 + i < n ? v[c8 * 8 + i] : 0.f);
+    *reinterpret_cast<uint4*>(tile + tc::kmajor_off(row, c8 * 8, KC)) = *reinterpret_cast<const uint4*>(h);
+  }
+}
+}  // namespace
+
+struct MlpSmem {
+  unsigned char w1t[64 * 16 * 2], w2t[64 * 64 * 2], w3t[64 * 64 * 2], w4t[16 * 64 * 2];
+  unsigned char w4[64 * 16 * 2], w3[64 * 64 * 2], w2[64 * 64 * 2];
+  unsigned char x0[128 * 16 * 2];              // a0, later dz4
+  unsigned char buf[2][128 * 64 * 2];          // activations / gradients, ping-pong
+  float b2[64], b3[64], b4[16];
+  double red[4];
+  uint64_t mbar;
+  uint32_t tslot;
+};
+
+__global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t mb = tc::smem_u32(&S.mbar);
+  // weights and biases (resident for all tiles)
+  load_kmajor(S.w1t, a.w1t, 64, 16);
+  load_kmajor(S.w2t, a.w2t, 64, 64);
+  load_kmajor(S.w3t, a.w3t, 64, 64);
+  load_kmajor(S.w4t, a.w4t, 16, 64);
+  const bool train = a.tau != nullptr;
+  if (train) {
+    load_kmajor(S.w4, a.w4, 64, 16);
+    load_kmajor(S.w3, a.w3, 64, 64);
+    load_kmajor(S.w2, a.w2, 64, 64);
+  }
+  for (int i = tid; i < 64; i += 128) {
+    S.b2[i] = a.b2[i];
+    S.b3[i] = a.b3[i];
+  }
+  if (tid < 16) S.b4[tid] = a.b4[tid];
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), 256);
+  if (tid == 0) tc::mbar_init(mb, 1);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = S.tslot;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's TMEM lanes
+  uint32_t phase = 0;
+  bool ok = true;
+  double loss = 0.0;
+  const uint32_t id64 = tc::idesc_bf16(128, 64), id16 = tc::idesc_bf16(128, 16);
+
+  // D[col0..] = A (KC columns, k_steps steps) * B^T; every thread waits.
+  auto mma = [&](uint32_t col0, const unsigned char* A, int KCa, const unsigned char* B, int KCb, int steps,
+                 uint32_t idesc) {
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid == 0) {
+      const uint32_t a0 = tc::smem_u32(A), b0 = tc::smem_u32(B);
+      for (int s = 0; s < steps; ++s)
+        tc::mma_bf16(tmem + col0, tc::smem_desc(a0 + 256 * s, 128, KCa * 16), tc::smem_desc(b0 + 256 * s, 128, KCb * 16),
+                     idesc, s > 0);
+      tc::commit(mb);
+    }
+    ok = __syncthreads_and(ok && tc::mbar_wait(mb, phase, MLP_WAIT)) != 0;  // block-uniform
+    phase ^= 1;
+    tc::fence_after_sync();
+  };
+  auto ld64 = [&](uint32_t col0, float (&v)[64]) {
+#pragma unroll
+    for (int c = 0; c < 64; c += 16) {
+      float t[16];
+      tc::tmem_ld16(lane_base + col0 + c, t);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[c + i] = t[i];
+    }
+  };
+  // feature-major bf16 row f of an [F][P] array
+  auto put_t = [&](__nv_bfloat16* dst, int f, long long p, float v) { dst[(long long)f * a.P + p] = __float2bfloat16_rn(v); };
+
+  for (int tile = blockIdx.x; tile * 128 < a.P && ok; tile += gridDim.x) {
+    const long long p = (long long)tile * 128 + tid;
+    const bool in = p < a.P;
+    // ---- forward ----
+    float v[64];
+    {
+      float x[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) x[i] = 0.f;
+      if (in) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) x[i] = a.x[p * 9 + i];
+      }
+      x[15] = in ? 1.f : 0.f;  // bias input of layer 1
+      store_row<16>(S.x0, tid, x, 16);
+      if (train && in) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) put_t(a.aT0, i, p, x[i]);
+      }
+    }
+    mma(0, S.x0, 16, S.w1t, 16, 1, id64);
+    ld64(0, v);
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = gelu(v[i]);
+    store_row<64>(S.buf[0], tid, v, 64);
+    if (train && in) {
+#pragma unroll 8
+      for (int i = 0; i < 64; ++i) put_t(a.aT1, i, p, v[i]);
+      put_t(a.aT1, 64, p, 1.f);
+    }
+    mma(64, S.buf[0], 64, S.w2t, 64, 4, id64);
+    ld64(64, v);
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = gelu(v[i] + S.b2[i]);
+    store_row<64>(S.buf[1], tid, v, 64);
+    if (train && in) {
+#pragma unroll 8
+      for (int i = 0; i < 64; ++i) put_t(a.aT2, i, p, v[i]);
+      put_t(a.aT2, 64, p, 1.f);
+    }
+    mma(128, S.buf[1], 64, S.w3t, 64, 4, id64);
+    ld64(128, v);
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = gelu(v[i] + S.b3[i]);
+    store_row<64>(S.buf[0], tid, v, 64);
+    if (train && in) {
+#pragma unroll 8
+      for (int i = 0; i < 64; ++i) put_t(a.aT3, i, p, v[i]);
+      put_t(a.aT3, 64, p, 1.f);
+    }
+    mma(192, S.buf[0], 64, S.w4t, 64, 4, id16);
+    float y[16];
+    tc::tmem_ld16(lane_base + 192, y);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) y[i] += S.b4[i];
+    if (in && a.y) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) a.y[p * 6 + i] = y[i];
+    }
+    if (!train) continue;
+    // ---- backward ----
+    float dz[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) dz[i] = 0.f;
+    if (in) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        const float r = y[i] - a.tau[p * 6 + i];
+        loss += (double)r * r;
+        dz[i] = 2.f * r * a.inv_count;
+      }
+    }
+    store_row<16>(S.x0, tid, dz, 16);
+    if (in) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) put_t(a.dzT4, i, p, dz[i]);
+    }
+    // dz_l from da_l (TMEM cols 192..255) and z_l (cols zcol..)
+    auto back = [&](uint32_t zcol, unsigned char* dst, __nv_bfloat16* dzT, const float* bias) {
+      float da[64], z[64];
+      ld64(192, da);
+      ld64(zcol, z);
+#pragma unroll
+      for (int i = 0; i < 64; ++i) da[i] *= gelu_d(z[i] + (bias ? bias[i] : 0.f));
+      if (dst) store_row<64>(dst, tid, da, 64);
+      if (in) {
+#pragma unroll 8
+        for (int i = 0; i < 64; ++i) put_t(dzT, i, p, da[i]);
+      }
+    };
+    mma(192, S.x0, 16, S.w4, 16, 1, id64);  // da3 = dz4 W4^T
+    back(128, S.buf[1], a.dzT3, S.b3);
+    mma(192, S.buf[1], 64, S.w3, 64, 4, id64);  // da2 = dz3 W3^T
+    back(64, S.buf[0], a.dzT2, S.b2);
+    mma(192, S.buf[0], 64, S.w2, 64, 4, id64);  // da1 = dz2 W2^T
+    back(0, nullptr, a.dzT1, nullptr);
+  }
+  if (!ok && tid == 0) atomicExch(a.err, 1);
+  if (train && a.loss) {  // per-CTA partial of sum (y - tau)^2
+    for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if (lane == 0) S.red[warp] = loss;
+    __syncthreads();
+    if (tid == 0) a.loss[blockIdx.x] = S.red[0] + S.red[1] + S.red[2] + S.red[3];
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
+size_t mlp_smem_bytes() { return sizeof(MlpSmem); }
+
+cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st) {
+  static bool ready = false;
+  if (!ready) {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+    if (e != cudaSuccess) return e;
+    ready = true;
+  }
+  k_mlp<<<grid, 128, sizeof(MlpSmem), st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace hit

@@ -207,7 +207,26 @@ template <typename T>
 cudaError_t launch_axpby(const V2<T>* x, T alpha, const V2<T>* y, T beta, V2<T>* out, long long n, cudaStream_t st);
 
 cudaError_t launch_tcgemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M,
-                          int N, int K, int* err, cudaStream_t st);
+                          int N, int K, int* err, cudaStream_t st, int splits = 1, float* work = nullptr);
+
+// Learned-closure MLP (k_mlp.cu).  Weights bf16 row-major: forward W^T of
+// layers 1-4 ([64][16], [64][64], [64][64], [16][64]; W1 row 15 of the input
+// holds b1) and backward W of layers 2-4 ([64][64], [64][64], [64][16]).
+struct MlpArgs {
+  const __nv_bfloat16 *w1t, *w2t, *w3t, *w4t, *w2, *w3, *w4;
+  const float *b2, *b3, *b4;
+  const float* x;    // [P][9]
+  const float* tau;  // [P][6] targets (NULL: inference only)
+  float* y;          // [P][6] outputs (may be NULL when training)
+  long long P;
+  float inv_count;   // 1 / (P * 6)
+  __nv_bfloat16 *aT0, *aT1, *aT2, *aT3;     // [16|65][P] activations (+ ones row)
+  __nv_bfloat16 *dzT1, *dzT2, *dzT3, *dzT4;  // [64|64|64|16][P]
+  double* loss;      // [grid] partial sums of (y - tau)^2
+  int* err;
+};
+size_t mlp_smem_bytes();
+cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st);
 
 struct SumArgs {
   const double* partial;

@@ -182,6 +182,38 @@ int hit_energy_budget(hit_plan *plan, const void *u_hat,
 int hit_tc_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C,
                      int ldc, int M, int N, int K, int *err_dev, void *stream);
 
+/* Learned subgrid-stress closure (north-star closure; no reference
+ * counterpart): pointwise MLP 9 -> 64 -> 64 -> 64 -> 6 with GELU, bf16 weights
+ * and activations, float32 accumulation, on the tcgen05 tensor cores.  Input
+ * per point: the 9 filtered velocity-gradient components du_i/dx_j (i-major);
+ * output: the 6 SGS stress components (xx, yy, zz, xy, xz, yz).  Weights are
+ * DEVICE bf16 row-major arrays: the forward operands W^T of layers 1-4
+ * ([64][16] with the layer-1 bias in input column 15, [64][64], [64][64],
+ * [16][64]) and, for training, W of layers 2-4 ([64][64], [64][64],
+ * [64][16]); biases b2, b3 ([64]) and b4 ([16]) float32. */
+typedef struct hit_mlp_weights {
+  const void *w1t, *w2t, *w3t, *w4t;
+  const void *w2, *w3, *w4;
+  const float *b2, *b3, *b4;
+} hit_mlp_weights;
+
+/* y[P][6] = MLP(x[P][9]) (DEVICE float32 arrays). */
+int hit_mlp_forward(const hit_mlp_weights *w, const float *x, int64_t P,
+                    float *y, int *err_dev, void *stream);
+
+/* Bytes of DEVICE workspace hit_mlp_train_grads needs for P points. */
+int64_t hit_mlp_workspace_bytes(int64_t P);
+
+/* Gradients of the mean-squared loss mean((MLP(x) - tau)^2) over P points
+ * (P a multiple of 16): dW1 [16][64] (row 15 = d b1), dW2 and dW3 [65][64]
+ * and dW4 [65][16] (row 64 = d b), float32 DEVICE arrays in [in][out]
+ * order; loss_dev (DEVICE double) receives the loss.  The weight gradients
+ * are tensor-core GEMMs over the points (split K). */
+int hit_mlp_train_grads(const hit_mlp_weights *w, const float *x,
+                        const float *tau, int64_t P, void *workspace,
+                        float *dW1, float *dW2, float *dW3, float *dW4,
+                        double *loss_dev, int *err_dev, void *stream);
+
 /* energy_spectrum without any device allocation.  No counterpart in the
  * reference: it serves callers that cannot allocate device memory -- code
  * running while its stream is being captured into a CUDA graph, an XLA custom

@@ -707,3 +707,58 @@ def rollout_vjp(grid, u0, params, dt, nsteps, ub, t0=0.0, checkpoint_every=None)
             ub, p = rk4_step_vjp(grid, seg[i], params, dt, ub, t0 + (i0 + i) * dt)
             pbar = _add_params(pbar, p)
     return ub, pbar
+
+
+# ---------------------------------------------------------------------------
+# Learned SGS closure MLP (no reference counterpart): 9 -> 64 -> 64 -> 64 -> 6,
+# GELU (erf form), restated with the tensor-core kernels' bf16 roundings (bf16
+# weights, inputs, hidden activations and backward gradients; float32 biases
+# and pre-activations; sums in float64), so the CUDA forward, loss and weight
+# gradients can be checked against it.
+# ---------------------------------------------------------------------------
+
+
+def bf16(x):
+    """Round float32 values to bfloat16 (nearest, ties to even), as float32."""
+    a = np.ascontiguousarray(np.asarray(x, np.float32))
+    b = a.view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) >> 16 << 16
+    return b.astype(np.uint32).view(np.float32).reshape(a.shape)
+
+
+def _gelu(x):
+    from scipy.special import erf
+    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+
+
+def _gelu_d(x):
+    from scipy.special import erf
+    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+
+
+def mlp_loss_grads(params, x, tau):
+    """params = (W1 [9,64], b1, W2 [64,64], b2, W3, b3, W4 [64,6], b4) float32;
+    x [P,9], tau [P,6].  Returns (y, loss, grads) with grads in the params'
+    order; loss = mean((y - tau)^2)."""
+    W1, b1, W2, b2, W3, b3, W4, b4 = [np.asarray(p, np.float32) for p in params]
+    P = x.shape[0]
+    f64 = np.float64
+    a0 = bf16(x).astype(f64)
+    z1 = a0 @ bf16(W1).astype(f64) + bf16(b1).astype(f64)
+    a1 = bf16(_gelu(z1.astype(np.float32))).astype(f64)
+    z2 = a1 @ bf16(W2).astype(f64) + b2
+    a2 = bf16(_gelu(z2.astype(np.float32))).astype(f64)
+    z3 = a2 @ bf16(W3).astype(f64) + b3
+    a3 = bf16(_gelu(z3.astype(np.float32))).astype(f64)
+    y = a3 @ bf16(W4).astype(f64) + b4
+    r = y - tau
+    loss = float(np.mean(r * r))
+    dz4 = bf16((2.0 * r / (P * 6)).astype(np.float32)).astype(f64)
+    da3 = dz4 @ bf16(W4).astype(f64).T
+    dz3 = bf16((da3 * _gelu_d(z3)).astype(np.float32)).astype(f64)
+    da2 = dz3 @ bf16(W3).astype(f64).T
+    dz2 = bf16((da2 * _gelu_d(z2)).astype(np.float32)).astype(f64)
+    da1 = dz2 @ bf16(W2).astype(f64).T
+    dz1 = bf16((da1 * _gelu_d(z1)).astype(np.float32)).astype(f64)
+    grads = (a0.T @ dz1, dz1.sum(0), a1.T @ dz2, dz2.sum(0), a2.T @ dz3, dz3.sum(0), a3.T @ dz4, dz4.sum(0))
+    return y, loss, grads

@@ -26,3 +26,75 @@ def test_tc_gemm_bf16(nat, M, N, K):
     ref = A.float() @ B.float().T
     assert int(err.item()) == 0
     assert torch.allclose(C, ref, rtol=1e-5, atol=1e-4 * float(ref.abs().max()))
+
+
+def _mlp_case(h3mod, P, seed):
+    closure = importlib.import_module("3dhit_b200.closure")
+    m = closure.ClosureMLP("cuda", seed=seed)
+    g = torch.Generator().manual_seed(seed + 1)
+    x = torch.randn(P, 9, generator=g) * 1.5
+    tau = torch.randn(P, 6, generator=g) * 0.5
+    return m, x, tau
+
+
+def _np_params(m):
+    return [t.detach().cpu().numpy() for t in m.params]
+
+
+def test_mlp_forward_matches_oracle(h3, orc):
+    m, x, tau = _mlp_case(h3, 1000, 3)
+    y = m.raw_forward(x.cuda()).cpu().numpy()
+    yo, _, _ = orc.mlp_loss_grads(_np_params(m), x.numpy(), tau.numpy())
+    m.check_errors()
+    import numpy as np
+    assert np.linalg.norm(y - yo) <= 1e-3 * np.linalg.norm(yo)
+
+
+def test_mlp_grads_match_oracle(h3, orc):
+    """Loss and all eight parameter gradients of the tensor-core training pass
+    against the oracle restatement with the same bf16 roundings."""
+    import numpy as np
+    m, x, tau = _mlp_case(h3, 4096, 5)
+    loss = float(m.loss_and_grads(x.cuda(), tau.cuda()).item())
+    m.check_errors()
+    _, lo, go = orc.mlp_loss_grads(_np_params(m), x.numpy(), tau.numpy())
+    assert abs(loss - lo) <= 1e-4 * lo
+    for p, ref in zip(m.params, go):
+        got = p.grad.cpu().numpy().astype(np.float64)
+        assert np.linalg.norm(got - ref) <= 1e-2 * np.linalg.norm(ref), (got.shape, np.linalg.norm(got - ref) / np.linalg.norm(ref))
+
+
+def test_mlp_grads_close_to_float32_autograd(h3):
+    """Against torch autograd of the same network in float32 (no bf16): equal
+    to the bf16 rounding of weights and activations."""
+    m, x, tau = _mlp_case(h3, 4096, 7)
+    m.loss_and_grads(x.cuda(), tau.cuda())
+    ps = [p.detach().clone().requires_grad_(True) for p in m.params]
+    W1, b1, W2, b2, W3, b3, W4, b4 = ps
+    gelu = torch.nn.functional.gelu
+    xc, tc_ = x.cuda(), tau.cuda()
+    y = gelu(gelu(gelu(xc @ W1 + b1) @ W2 + b2) @ W3 + b3) @ W4 + b4
+    loss = ((y - tc_) ** 2).mean()
+    loss.backward()
+    for p, q in zip(m.params, ps):
+        assert torch.linalg.vector_norm(p.grad - q.grad) <= 5e-2 * torch.linalg.vector_norm(q.grad)
+
+
+def test_mlp_training_reduces_loss(h3):
+    """A few Adam steps on the tensor-core gradients fit a smooth target."""
+    closure = importlib.import_module("3dhit_b200.closure")
+    m = closure.ClosureMLP("cuda", seed=11)
+    g = torch.Generator().manual_seed(12)
+    x = (torch.randn(8192, 9, generator=g)).cuda()
+    tau = torch.stack([x[:, 0] * x[:, 4], x[:, 1] + x[:, 3], x[:, 8] ** 2, torch.tanh(x[:, 2]), x[:, 5] * 0.5,
+                       x[:, 6] - x[:, 7]], 1) * 0.3
+    for p in m.params:
+        p.requires_grad_(True)
+    opt = torch.optim.Adam(m.params, lr=3e-3)
+    losses = []
+    for it in range(300):
+        losses.append(float(m.loss_and_grads(x, tau).item()))
+        opt.step()
+        m.pack()
+    m.check_errors()
+    assert losses[-1] < 0.2 * losses[0], (losses[0], losses[-1])
