@@ -51,6 +51,7 @@ class ClosureMLP:
         self._err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._ws = None
         self._packed = None
+        self._physical = None
 
     @property
     def params(self):
@@ -104,6 +105,31 @@ class ClosureMLP:
     def __call__(self, grads):
         """SGS stress [P, 6] from velocity gradients [P, 9] (physical units)."""
         return self.raw_forward(grads / self.x_scale) * self.y_scale
+
+    def pack_physical(self):
+        """bf16 operands with the normalisation folded in (x / x_scale into W1,
+        y_scale into W4 and b4): the network maps physical gradients to the
+        physical stress."""
+        W1, W4, b4 = self.W1, self.W4, self.b4
+        self.W1 = W1 / self.x_scale[:, None]
+        self.W4, self.b4 = W4 * self.y_scale[None, :], b4 * self.y_scale
+        try:
+            w = self.pack()
+        finally:
+            self.W1, self.W4, self.b4 = W1, W4, b4
+        self._physical = self._packed
+        self._packed = None
+        return w
+
+    def forward_fields(self, grads, out):
+        """SGS stress fields out (6, P) from gradient fields grads (9, P)
+        (component-major, physical units, float32 device tensors)."""
+        if getattr(self, "_physical", None) is None:
+            self.pack_physical()
+        P = grads.shape[1]
+        nat.call("hit_mlp_forward_strided", ctypes_ref(self._physical[0]), nat.ptr(grads), P, 1, P, nat.ptr(out), P, 1,
+                 nat.ptr(self._err), nat.stream_ptr(self.device))
+        return out
 
     def loss_and_grads(self, x, tau):
         """Mean-squared loss of the network on normalised (x, tau) and the

@@ -293,3 +293,69 @@ template cudaError_t launch_axpby<double>(const double2*, double, const double2*
                                           cudaStream_t);
 
 }  // namespace hit
+
+namespace hit {
+// ---------------------------------------------------------------------------
+// LES with the learned closure (no reference counterpart)
+// ---------------------------------------------------------------------------
+
+// g[3i + j] = 1j k_j u_i (spectral velocity gradients, 9 components)
+template <typename T>
+__global__ void __launch_bounds__(NT) k_grad9(const V2<T>* __restrict__ u, V2<T>* __restrict__ g, Geom gm, KTab<T> kt) {
+  const long long nm = (long long)gm.Nx * gm.Ny * gm.Nzh;
+  for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < nm; m += (long long)gridDim.x * NT) {
+    const int z = (int)(m % gm.Nzh);
+    const long long r = m / gm.Nzh;
+    const int fy = (int)(r % gm.Ny), fx = (int)(r / gm.Ny);
+    const T k[3] = {kt.kx[fx], kt.ky[fy], kt.kz[z]};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const V2<T> ui = u[i * nm + m];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) g[(3 * i + j) * nm + m] = cmul_i(cscale(ui, k[j]));
+    }
+  }
+}
+
+// du += project(dealias(-1j k_j tau_ij)), tau in the order xx, yy, zz, xy, xz, yz
+template <typename T>
+__global__ void __launch_bounds__(NT) k_sgs_force(const V2<T>* __restrict__ t, V2<T>* __restrict__ du, Geom gm,
+                                                  KTab<T> kt) {
+  const long long nm = (long long)gm.Nx * gm.Ny * gm.Nzh;
+  for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < nm; m += (long long)gridDim.x * NT) {
+    int fx, fy, z;
+    const Mode<T> d = mode_of(m, gm, kt, fx, fy, z);
+    const V2<T> xx = t[m], yy = t[nm + m], zz = t[2 * nm + m], xy = t[3 * nm + m], xz = t[4 * nm + m],
+                yz = t[5 * nm + m];
+    V2<T> f[3];
+    // k_j tau_ij, then times -1j
+    V2<T> s0, s1, s2;
+    s0.x = d.kx * xx.x + d.ky * xy.x + d.kz * xz.x;
+    s0.y = d.kx * xx.y + d.ky * xy.y + d.kz * xz.y;
+    s1.x = d.kx * xy.x + d.ky * yy.x + d.kz * yz.x;
+    s1.y = d.kx * xy.y + d.ky * yy.y + d.kz * yz.y;
+    s2.x = d.kx * xz.x + d.ky * yz.x + d.kz * zz.x;
+    s2.y = d.kx * xz.y + d.ky * yz.y + d.kz * zz.y;
+    f[0] = cmul_mi(s0);
+    f[1] = cmul_mi(s1);
+    f[2] = cmul_mi(s2);
+    proj_mask(d, f);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) du[c * nm + m] = cadd(du[c * nm + m], f[c]);
+  }
+}
+
+template <typename T> cudaError_t launch_grad9(const V2<T>* u, V2<T>* g, const Geom& gm, KTab<T> kt, cudaStream_t st) {
+  k_grad9<T><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(u, g, gm, kt);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_sgs_force(const V2<T>* t, V2<T>* du, const Geom& gm, KTab<T> kt, cudaStream_t st) {
+  k_sgs_force<T><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(t, du, gm, kt);
+  return cudaGetLastError();
+}
+template cudaError_t launch_grad9<float>(const float2*, float2*, const Geom&, KTab<float>, cudaStream_t);
+template cudaError_t launch_grad9<double>(const double2*, double2*, const Geom&, KTab<double>, cudaStream_t);
+template cudaError_t launch_sgs_force<float>(const float2*, float2*, const Geom&, KTab<float>, cudaStream_t);
+template cudaError_t launch_sgs_force<double>(const double2*, double2*, const Geom&, KTab<double>, cudaStream_t);
+}  // namespace hit

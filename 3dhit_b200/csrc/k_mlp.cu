@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
       for (int i = 0; i < 16; ++i) x[i] = 0.f;
       if (in) {
 #pragma unroll
-        for (int i = 0; i < 9; ++i) x[i] = a.x[p * 9 + i];
+        for (int i = 0; i < 9; ++i) x[i] = a.x[i * a.x_sf + p * a.x_sp];
       }
       x[15] = in ? 1.f : 0.f;  // bias input of layer 1
       store_row<16>(S.x0, tid, x, 16);
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
     for (int i = 0; i < 6; ++i) y[i] += S.b4[i];
     if (in && a.y) {
 #pragma unroll
-      for (int i = 0; i < 6; ++i) a.y[p * 6 + i] = y[i];
+      for (int i = 0; i < 6; ++i) a.y[i * a.y_sf + p * a.y_sp] = y[i];
     }
     if (!train) continue;
     // ---- backward ----

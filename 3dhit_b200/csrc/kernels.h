@@ -205,6 +205,9 @@ template <typename T> cudaError_t launch_adj_cross(T* p, long long n, cudaStream
 template <typename T> cudaError_t launch_adj_combine(const AdjArgs<T>& a, cudaStream_t st);
 template <typename T>
 cudaError_t launch_axpby(const V2<T>* x, T alpha, const V2<T>* y, T beta, V2<T>* out, long long n, cudaStream_t st);
+template <typename T> cudaError_t launch_grad9(const V2<T>* u, V2<T>* g, const Geom& gm, KTab<T> kt, cudaStream_t st);
+template <typename T>
+cudaError_t launch_sgs_force(const V2<T>* t, V2<T>* du, const Geom& gm, KTab<T> kt, cudaStream_t st);
 
 cudaError_t launch_tcgemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M,
                           int N, int K, int* err, cudaStream_t st, int splits = 1, float* work = nullptr);
@@ -215,10 +218,10 @@ cudaError_t launch_tcgemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* 
 struct MlpArgs {
   const __nv_bfloat16 *w1t, *w2t, *w3t, *w4t, *w2, *w3, *w4;
   const float *b2, *b3, *b4;
-  const float* x;    // [P][9]
+  const float* x;    // feature f of point p at x[f * x_sf + p * x_sp]
   const float* tau;  // [P][6] targets (NULL: inference only)
-  float* y;          // [P][6] outputs (may be NULL when training)
-  long long P;
+  float* y;          // output c of point p at y[c * y_sf + p * y_sp] (may be NULL when training)
+  long long P, x_sf, x_sp, y_sf, y_sp;
   float inv_count;   // 1 / (P * 6)
   __nv_bfloat16 *aT0, *aT1, *aT2, *aT3;     // [16|65][P] activations (+ ones row)
   __nv_bfloat16 *dzT1, *dzT2, *dzT3, *dzT4;  // [64|64|64|16][P]

@@ -56,17 +56,26 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 extern "C" {
 
-int hit_mlp_forward(const hit_mlp_weights* w, const float* x, int64_t P, float* y, int* err, void* stream) {
+int hit_mlp_forward_strided(const hit_mlp_weights* w, const float* x, int64_t x_sf, int64_t x_sp, int64_t P, float* y,
+                            int64_t y_sf, int64_t y_sp, int* err, void* stream) {
   if (!weights_ok(w, false) || !x || !y || !err) return hit::record_error(HIT_E_INVALID, "mlp_forward: NULL argument");
   if (P < 1) return hit::record_error(HIT_E_INVALID, "mlp_forward: P must be >= 1");
   MlpArgs a = args_of(w);
   a.x = x;
   a.y = y;
   a.P = P;
+  a.x_sf = x_sf;
+  a.x_sp = x_sp;
+  a.y_sf = y_sf;
+  a.y_sp = y_sp;
   a.err = err;
   const int grid = (int)std::min<int64_t>((P + 127) / 128, MLP_GRID);
   cudaError_t e = hit::launch_mlp(a, grid, (cudaStream_t)stream);
   return e == cudaSuccess ? HIT_OK : cuda_err(e, "mlp_forward");
+}
+
+int hit_mlp_forward(const hit_mlp_weights* w, const float* x, int64_t P, float* y, int* err, void* stream) {
+  return hit_mlp_forward_strided(w, x, 1, 9, P, y, 1, 6, err, stream);
 }
 
 int64_t hit_mlp_workspace_bytes(int64_t P) {
@@ -84,6 +93,8 @@ int hit_mlp_train_grads(const hit_mlp_weights* w, const float* x, const float* t
   cudaStream_t st = (cudaStream_t)stream;
   MlpArgs a = args_of(w);
   a.x = x;
+  a.x_sf = 1;
+  a.x_sp = 9;
   a.tau = tau;
   a.P = P;
   a.inv_count = (float)(1.0 / ((double)P * 6.0));

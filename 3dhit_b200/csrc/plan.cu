@@ -914,14 +914,14 @@ int hit_plan_num_shells(const hit_plan* p) { return p ? p->smax : 0; }
 
 int hit_to_physical(hit_plan* p, const void* u_hat, int nc, void* u, void* stream) {
   if (!p || !u_hat || !u) return fail(HIT_E_INVALID, "NULL argument");
-  if (nc < 1 || nc > 6) return fail(HIT_E_INVALID, "ncomp must be in [1, 6]");
+  if (nc < 1 || nc > 9) return fail(HIT_E_INVALID, "ncomp must be in [1, 9]");
   DeviceGuard dg(p->device);
   return DISPATCH(p, to_physical_impl)(p, u_hat, nc, u, (cudaStream_t)stream);
 }
 
 int hit_to_spectral(hit_plan* p, const void* u, int nc, void* u_hat, void* stream) {
   if (!p || !u_hat || !u) return fail(HIT_E_INVALID, "NULL argument");
-  if (nc < 1 || nc > 6) return fail(HIT_E_INVALID, "ncomp must be in [1, 6]");
+  if (nc < 1 || nc > 9) return fail(HIT_E_INVALID, "ncomp must be in [1, 9]");
   DeviceGuard dg(p->device);
   return DISPATCH(p, to_spectral_impl)(p, u, nc, u_hat, (cudaStream_t)stream);
 }
@@ -1037,6 +1037,35 @@ int hit_rollout_vjp(hit_plan* p, const void* u0, const hit_params* pr, double dt
   DeviceGuard dg(p->device);
   const int K = (int)std::min<int64_t>(checkpoint_every, std::max<int64_t>(nsteps, 1));
   return DISPATCH(p, vjp_entry)(p, 2, u0, pr, dt, nsteps, K, ct, u0_bar, param_ct, (cudaStream_t)stream);
+}
+
+int hit_velocity_gradients(hit_plan* p, const void* u_hat, void* grads, void* stream) {
+  if (!p || !u_hat || !grads) return fail(HIT_E_INVALID, "NULL argument");
+  DeviceGuard dg(p->device);
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  const size_t es = p->dtype == HIT_DTYPE_F32 ? sizeof(float2) : sizeof(double2);
+  int rc;
+  if ((rc = ensure(p->ax9, 9 * (size_t)g.Nx * g.Ny * g.Nzh * es))) return rc;
+  cudaError_t e = p->dtype == HIT_DTYPE_F32
+                      ? launch_grad9<float>(static_cast<const float2*>(u_hat), static_cast<float2*>(p->ax9.p), g,
+                                            ktab_of<float>(p), (cudaStream_t)stream)
+                      : launch_grad9<double>(static_cast<const double2*>(u_hat), static_cast<double2*>(p->ax9.p), g,
+                                             ktab_of<double>(p), (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "velocity_gradients");
+  return DISPATCH(p, to_physical_impl)(p, p->ax9.p, 9, grads, (cudaStream_t)stream);
+}
+
+int hit_add_sgs_force(hit_plan* p, const void* tau_hat, void* du, void* stream) {
+  if (!p || !tau_hat || !du) return fail(HIT_E_INVALID, "NULL argument");
+  DeviceGuard dg(p->device);
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  cudaError_t e = p->dtype == HIT_DTYPE_F32
+                      ? launch_sgs_force<float>(static_cast<const float2*>(tau_hat), static_cast<float2*>(du), g,
+                                                ktab_of<float>(p), (cudaStream_t)stream)
+                      : launch_sgs_force<double>(static_cast<const double2*>(tau_hat), static_cast<double2*>(du), g,
+                                                 ktab_of<double>(p), (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "add_sgs_force");
+  return HIT_OK;
 }
 
 int hit_tc_gemm_bf16(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M, int N, int K, int* err,

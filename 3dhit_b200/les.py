@@ -1,0 +1,246 @@
+"""Coarse LES with the learned subgrid-stress closure.
+
+* ``box_filter``: sharp spectral filter of a fine state to the coarse grid's
+  2/3 box (|n_i| <= Nc/3), with the (Nc/Nf)^3 rescale of the unnormalised
+  transform, giving the coarse spectral state of the filtered field.
+* ``velocity_gradients``: du_i/dx_j of a state at its grid points (9 fields,
+  ``hit_velocity_gradients``), the closure's input.
+* ``sgs_stress``: the exact SGS stress of a fine state on the coarse grid,
+  tau_ij = F(u_i u_j) - F(u_i) F(u_j) (xx, yy, zz, xy, xz, yz), the training
+  target.
+* ``LESRHS``: the coarse RHS, the fused Navier-Stokes RHS plus
+  project(dealias(-d_j tau_ij)) of the closure's stress (``hit_add_sgs_force``);
+  without a closure it is the unmodelled coarse solver.
+* ``make_dataset`` / ``train`` / ``run_les``: the closure experiment
+  (filtered forced DNS -> training -> LES against filtered DNS spectra).
+
+The reference has no LES; this is the north star's learned part built on the
+package's own solver and kernels.
+"""
+
+from __future__ import annotations
+
+import time
+
+import torch
+
+from . import _native as nat
+from .closure import ClosureMLP
+from .diagnostics import energy_spectrum, energy_budget
+from .fields import cfl_dt, hit_initial_field
+from .forcing import HoldEnergyForcing, LinearForcing
+from .grid import _check_state, make_grid, to_physical, to_spectral
+from .integrators import rk4_step, rollout
+from .navierstokes import NSParams, make_ns_rhs
+
+__all__ = ["box_filter", "velocity_gradients", "sgs_stress", "LESRHS", "make_dataset", "train", "run_les"]
+
+_PAIRS = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+
+
+def _box_index(Nf, Nc, kc, device):
+    src = torch.cat([torch.arange(0, kc + 1), torch.arange(Nf - kc, Nf)]).to(device)
+    dst = torch.cat([torch.arange(0, kc + 1), torch.arange(Nc - kc, Nc)]).to(device)
+    return src, dst
+
+
+def box_filter(f_hat, fine, coarse):
+    """Coarse spectral fields (any number of leading components) of the fine
+    spectral fields ``f_hat`` restricted to |n_i| <= Nc/3."""
+    kc = min(coarse.Nx, coarse.Ny, coarse.Nz) // 3
+    lead = f_hat.shape[:-3]
+    out = torch.zeros(*lead, coarse.Nx, coarse.Ny, coarse.Nz // 2 + 1, dtype=f_hat.dtype, device=f_hat.device)
+    sx, dx = _box_index(fine.Nx, coarse.Nx, kc, f_hat.device)
+    sy, dy = _box_index(fine.Ny, coarse.Ny, kc, f_hat.device)
+    scale = (coarse.Nx * coarse.Ny * coarse.Nz) / (fine.Nx * fine.Ny * fine.Nz)
+    sub = f_hat[..., :, :, : kc + 1].index_select(-3, sx).index_select(-2, sy)
+    tmp = torch.zeros(*lead, coarse.Nx, sub.shape[-2], kc + 1, dtype=f_hat.dtype, device=f_hat.device)
+    tmp.index_copy_(-3, dx, sub)
+    tmp2 = torch.zeros(*lead, coarse.Nx, coarse.Ny, kc + 1, dtype=f_hat.dtype, device=f_hat.device)
+    tmp2.index_copy_(-2, dy, tmp)
+    out[..., : kc + 1] = tmp2 * scale
+    return out
+
+
+def velocity_gradients(u_hat, grid):
+    """du_i/dx_j (component 3i + j) at the grid points, shape (9, N^3)."""
+    u_hat = _check_state(u_hat, grid)
+    P = grid.Nx * grid.Ny * grid.Nz
+    g = torch.empty(9, P, dtype=grid.dtype, device=grid.device)
+    nat.call("hit_velocity_gradients", grid.plan.handle, nat.ptr(u_hat), nat.ptr(g), nat.stream_ptr(grid.device))
+    return g
+
+
+def sgs_stress(u_hat_fine, fine, coarse):
+    """Exact SGS stress of the filter on the coarse grid, shape (6, Nc^3)."""
+    u = to_physical(u_hat_fine, fine)
+    prods = torch.stack([u[i] * u[j] for i, j in _PAIRS])
+    del u
+    fuu = to_physical(box_filter(to_spectral(prods, fine), fine, coarse), coarse)
+    ub = to_physical(box_filter(u_hat_fine, fine, coarse), coarse)
+    tau = torch.stack([fuu[c] - ub[i] * ub[j] for c, (i, j) in enumerate(_PAIRS)])
+    return tau.reshape(6, -1)
+
+
+class LESRHS:
+    """Coarse RHS with an optional learned closure (``ClosureMLP``)."""
+
+    def __init__(self, grid, closure=None):
+        self.grid = grid
+        self.ns = make_ns_rhs(grid)
+        self.closure = closure
+        self._tau = None
+
+    def __call__(self, u_hat, params, t):
+        g = self.grid
+        du = self.ns(u_hat, params, t, assume_dealiased=True)
+        if self.closure is not None:
+            P = g.Nx * g.Ny * g.Nz
+            grads = velocity_gradients(u_hat, g)
+            if self._tau is None:
+                self._tau = torch.empty(6, P, dtype=g.dtype, device=g.device)
+            self.closure.forward_fields(grads, self._tau)
+            tau_hat = to_spectral(self._tau.reshape(6, g.Nx, g.Ny, g.Nz), g)
+            nat.call("hit_add_sgs_force", g.plan.handle, nat.ptr(tau_hat), nat.ptr(du), nat.stream_ptr(g.device))
+        return du
+
+
+def _spectrum(u_hat, grid, kmax):
+    _, E = energy_spectrum(u_hat, grid)
+    return torch.as_tensor(E[:kmax], dtype=torch.float64)
+
+
+def make_dataset(fine_n=256, coarse_n=64, nu=1.5e-3, E_target=1.5, spinup=2000, snapshots=200, every=50, seed=0,
+                 device="cuda", log=None):
+    """Hold-energy (Lundgren) forced DNS on fine_n^3, filtered to coarse_n^3:
+    features (S, 9, Pc) velocity gradients of the filtered field, targets
+    (S, 6, Pc) the SGS stress, the filtered spectra, the forcing coefficient
+    and the DNS step time."""
+    fine = make_grid(fine_n, device=device)
+    coarse = make_grid(coarse_n, device=device)
+    forcing = HoldEnergyForcing(E_target, nu)
+    p = NSParams(nu=nu, forcing=forcing)
+    rhs = make_ns_rhs(fine)
+    u = hit_initial_field(seed, fine)
+    dt = cfl_dt(u, fine, 0.5)
+    t0 = time.perf_counter()
+    u = rollout(rhs, u, p, dt, spinup, assume_dealiased=True)
+    torch.cuda.synchronize()
+    Pc = coarse.Nx * coarse.Ny * coarse.Nz
+    X = torch.empty(snapshots, 9, Pc, device=device)
+    Y = torch.empty(snapshots, 6, Pc, device=device)
+    spectra, A = [], []
+    u0_coarse = None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dns_ms = 0.0
+    kc = coarse_n // 3
+    for s in range(snapshots):
+        e0.record()
+        u = rollout(rhs, u, p, dt, every, assume_dealiased=True)
+        e1.record()
+        torch.cuda.synchronize()
+        dns_ms += e0.elapsed_time(e1)
+        ub = box_filter(u, fine, coarse)
+        if u0_coarse is None:
+            u0_coarse = ub.clone()
+        X[s] = velocity_gradients(ub, coarse)
+        Y[s] = sgs_stress(u, fine, coarse)
+        spectra.append(_spectrum(ub, coarse, kc))
+        b = energy_budget(u, fine, nu, forcing)
+        A.append(float(b["eps"]) / (2.0 * float(b["E"])))  # hold-energy A = 2 nu Omega / 2E
+        if log and s % 20 == 0:
+            log(f"snapshot {s}: E={float(b['E']):.4f}")
+    return dict(X=X, Y=Y, spectra=torch.stack(spectra), A=A, dt=dt, nu=nu, dns_ms_per_step=dns_ms / (snapshots * every),
+                u0_coarse=u0_coarse, fine=fine, coarse=coarse, wall_s=time.perf_counter() - t0)
+
+
+def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20, log=None):
+    """Fit the closure on (X, Y) with Adam on the tensor-core gradients; the
+    last ``val_snapshots`` snapshots are held out.  Returns the model and the
+    loss history (train, validation)."""
+    X, Y = data["X"], data["Y"]
+    S = X.shape[0]
+    ntr = S - val_snapshots
+    m = ClosureMLP(X.device, seed=seed)
+    m.x_scale = X[:ntr].transpose(0, 1).reshape(9, -1).std(1)
+    m.y_scale = Y[:ntr].transpose(0, 1).reshape(6, -1).std(1)
+    for q in m.params:
+        q.requires_grad_(True)
+    opt = torch.optim.Adam(m.params, lr=lr)
+    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, steps)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    hist = []
+    xs, ys = m.x_scale.view(1, 9, 1), m.y_scale.view(1, 6, 1)
+
+    def batch(idx):
+        xb = (X[idx] / xs).permute(0, 2, 1).reshape(-1, 9).contiguous()
+        yb = (Y[idx] / ys).permute(0, 2, 1).reshape(-1, 6).contiguous()
+        return xb, yb
+
+    val = batch(torch.arange(ntr, S, device=X.device))
+    for it in range(steps):
+        idx = torch.randperm(ntr, generator=g)[:batch_snapshots].to(X.device)
+        xb, yb = batch(idx)
+        loss = m.loss_and_grads(xb, yb)
+        opt.step()
+        sched.step()
+        m.pack()
+        if it % 50 == 0 or it == steps - 1:
+            vy = m.raw_forward(val[0])
+            vl = float(((vy - val[1]) ** 2).mean())
+            hist.append((it, float(loss.item()), vl))
+            if log:
+                log(f"step {it}: train {hist[-1][1]:.4f} val {vl:.4f}")
+    m.check_errors()
+    return m, hist
+
+
+def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True):
+    """Coarse LES from the first filtered snapshot's state, Lundgren forcing at
+    the DNS's mean coefficient; returns the time-averaged spectrum over the
+    samples after ``discard`` steps, the step time and the energy history."""
+    coarse = data["coarse"]
+    dev = coarse.device
+    kc = coarse.Nx // 3
+    A = sum(data["A"]) / len(data["A"])
+    p = NSParams(nu=data["nu"], forcing=LinearForcing(A))
+    rhs = LESRHS(coarse, closure)
+    u = data["u0_coarse"].clone()
+    dt = data.get("dt_les") or cfl_dt(u, coarse, 0.5)
+
+    def step(x):
+        return rk4_step(rhs, x, p, dt, 0.0)
+
+    run = step
+    if graph:
+        static = u.clone()
+        for _ in range(3):
+            out = step(static)
+        torch.cuda.synchronize()
+        gph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gph):
+            out = step(static)
+
+        def run(x):
+            static.copy_(x)
+            gph.replay()
+            return out.clone()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    spec, n, energies = torch.zeros(kc, dtype=torch.float64), 0, []
+    for i in range(1, steps + 1):
+        u = run(u)
+        if i % sample_every == 0:
+            s = _spectrum(u, coarse, kc)
+            energies.append(float(s.sum()))
+            if i > discard:
+                spec += s
+                n += 1
+    torch.cuda.synchronize()
+    # timing: a clean window of 200 steps
+    e0.record()
+    for _ in range(200):
+        u = run(u)
+    e1.record()
+    torch.cuda.synchronize()
+    return dict(spectrum=spec / max(n, 1), ms_per_step=e0.elapsed_time(e1) / 200, dt=dt, energies=energies,
+                finite=bool(torch.isfinite(u).all()))

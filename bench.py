@@ -300,6 +300,52 @@ def run_adjoint(args):
     return 0
 
 
+def run_closure(args):
+    """Learned SGS closure (Lundgren hold-energy forced DNS on F^3, sharp
+    spectral filter to C^3 at k_c = C/3, MLP 9 -> 64x3 -> 6 on the tensor
+    cores, then C^3 LES from the first filtered snapshot with Lundgren forcing
+    at the DNS's mean coefficient, with and without the closure).  Prints one
+    JSON line: E(k) errors against the time-averaged filtered DNS spectrum for
+    k <= k_c, and the wall-time ratio of the DNS to the LES over the same
+    physical time."""
+    les = importlib.import_module("3dhit_b200.les")
+
+    def log(msg):
+        print(msg, file=sys.stderr, flush=True)
+
+    t0 = time.perf_counter()
+    data = les.make_dataset(fine_n=args.cl_fine, coarse_n=args.cl_coarse, spinup=args.cl_spinup,
+                            snapshots=args.cl_snapshots, every=args.cl_every, log=log)
+    t_data = time.perf_counter() - t0
+    model, hist = les.train(data, steps=args.cl_train_steps, val_snapshots=max(1, args.cl_snapshots // 10), log=log)
+    t_train = time.perf_counter() - t0 - t_data
+    ref = data["spectra"].mean(0)
+    kc = data["coarse"].Nx // 3
+    out = {}
+    for name, cl in (("no_closure", None), ("closure", model)):
+        r = les.run_les(data, cl, steps=args.cl_les_steps, discard=args.cl_les_steps // 5)
+        rel = (r["spectrum"] / ref - 1).abs()
+        T = args.cl_les_steps * r["dt"]
+        dns_wall = T / data["dt"] * data["dns_ms_per_step"]
+        out[name] = {"max_rel_err_Ek": float(rel.max()), "mean_rel_err_Ek": float(rel.mean()),
+                     "rel_err_Ek": [round(float(x), 4) for x in rel], "ms_per_step": r["ms_per_step"],
+                     "dt": r["dt"], "finite": r["finite"], "wall_ratio_dns_over_les": dns_wall / (args.cl_les_steps *
+                                                                                                r["ms_per_step"]),
+                     "energy_first_last": [r["energies"][0], r["energies"][-1]] if r["energies"] else None}
+    line = {"metric": f"closure-LES {args.cl_coarse}^3 vs filtered {args.cl_fine}^3 DNS: max E(k) rel err, k<=k_c",
+            "value": out["closure"]["max_rel_err_Ek"], "unit": "fraction", "higher_is_better": False,
+            "fallback_value": out["no_closure"]["max_rel_err_Ek"],
+            "config": {"workload": f"Lundgren hold-E DNS {args.cl_fine}^3 (nu=1.5e-3, E_t=1.5, CFL 0.5), "
+                                   f"{args.cl_spinup} spin-up steps, {args.cl_snapshots} snapshots every "
+                                   f"{args.cl_every} steps, filter k_c={kc}; MLP 9->64->64->64->6 GELU bf16; "
+                                   f"LES {args.cl_les_steps} steps, Lundgren forcing at the DNS mean A"},
+            "dns_ms_per_step": data["dns_ms_per_step"], "dns_dt": data["dt"], "mean_A": sum(data["A"]) / len(data["A"]),
+            "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train},
+            "no_closure": out["no_closure"], "closure": out["closure"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,11 +363,21 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=400)
     ap.add_argument("--adj-ckpt", type=int, default=20)
     ap.add_argument("--adj-dirs", type=int, default=8)
+    ap.add_argument("--closure", action="store_true", help="learned-closure LES experiment instead of the benchmark")
+    ap.add_argument("--cl-fine", type=int, default=256)
+    ap.add_argument("--cl-coarse", type=int, default=64)
+    ap.add_argument("--cl-spinup", type=int, default=2000)
+    ap.add_argument("--cl-snapshots", type=int, default=200)
+    ap.add_argument("--cl-every", type=int, default=50)
+    ap.add_argument("--cl-train-steps", type=int, default=400)
+    ap.add_argument("--cl-les-steps", type=int, default=5000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.adjoint:
         return run_adjoint(args)
+    if args.closure:
+        return run_closure(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -200,6 +200,22 @@ typedef struct hit_mlp_weights {
 /* y[P][6] = MLP(x[P][9]) (DEVICE float32 arrays). */
 int hit_mlp_forward(const hit_mlp_weights *w, const float *x, int64_t P,
                     float *y, int *err_dev, void *stream);
+/* The same with strided arrays: feature f of point p at x[f*x_sf + p*x_sp],
+ * output c at y[c*y_sf + p*y_sp] (component-major fields: x_sf = P, x_sp = 1). */
+int hit_mlp_forward_strided(const hit_mlp_weights *w, const float *x,
+                            int64_t x_sf, int64_t x_sp, int64_t P, float *y,
+                            int64_t y_sf, int64_t y_sp, int *err_dev,
+                            void *stream);
+
+/* LES with the closure (no reference counterpart), reference layout:
+ * grads_out (DEVICE, 9 x Nx*Ny*Nz, the plan's dtype) receives du_i/dx_j
+ * (component 3i + j) at the grid points of the state u_hat;
+ * hit_add_sgs_force adds project(dealias(-1j k_j tau_hat_ij)) to du_hat, tau_hat
+ * holding the 6 spectral components xx, yy, zz, xy, xz, yz. */
+int hit_velocity_gradients(hit_plan *plan, const void *u_hat, void *grads_out,
+                           void *stream);
+int hit_add_sgs_force(hit_plan *plan, const void *tau_hat, void *du_hat,
+                      void *stream);
 
 /* Bytes of DEVICE workspace hit_mlp_train_grads needs for P points. */
 int64_t hit_mlp_workspace_bytes(int64_t P);

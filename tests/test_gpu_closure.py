@@ -98,3 +98,56 @@ def test_mlp_training_reduces_loss(h3):
         m.pack()
     m.check_errors()
     assert losses[-1] < 0.2 * losses[0], (losses[0], losses[-1])
+
+
+def test_les_pieces_against_torch(h3):
+    """Velocity gradients, the SGS force and the box filter of the LES path
+    against torch references of the same spectral formulas."""
+    les = importlib.import_module("3dhit_b200.les")
+    g = h3.make_grid(32, dtype=torch.float64)
+    u = h3.random_field(3, g)
+    # gradients: irfftn(1j k_j u_i)
+    grads = les.velocity_gradients(u, g)
+    ks = [g.kx, g.ky, g.kz]
+    ref = torch.stack([h3.to_physical(1j * ks[j] * u[i], g).reshape(-1) for i in range(3) for j in range(3)])
+    assert torch.allclose(grads, ref, rtol=0, atol=1e-12 * float(ref.abs().max()))
+    # SGS force: du += project(dealias(-1j k_j tau_ij))
+    tau = torch.randn(6, 32, 32, 32, dtype=torch.float64, device="cuda")
+    th = h3.to_spectral(tau, g)
+    du = torch.zeros_like(u)
+    import importlib as il
+    nat = il.import_module("3dhit_b200._native")
+    nat.call("hit_add_sgs_force", g.plan.handle, nat.ptr(th), nat.ptr(du), nat.stream_ptr(g.device))
+    T = [[th[0], th[3], th[4]], [th[3], th[1], th[5]], [th[4], th[5], th[2]]]
+    f = torch.stack([-1j * (ks[0] * T[i][0] + ks[1] * T[i][1] + ks[2] * T[i][2]) for i in range(3)])
+    refd = h3.project(h3.dealias(f, g), g)
+    assert torch.allclose(du, refd, rtol=0, atol=1e-12 * float(refd.abs().max()))
+    # box filter of a field inside the coarse box: the same physical field at the coarse points
+    gf = h3.make_grid(32, dtype=torch.float64)
+    gc = h3.make_grid(16, dtype=torch.float64)
+    uf = h3.random_field(4, gf)
+    uc = les.box_filter(uf, gf, gc)
+    xf = h3.to_physical(h3.dealias(uf * (torch.sqrt(gf.k2) <= 5).to(uf.dtype), gf), gf)
+    uc5 = les.box_filter(h3.dealias(uf * (torch.sqrt(gf.k2) <= 5).to(uf.dtype), gf), gf, gc)
+    xc = h3.to_physical(uc5, gc)
+    assert torch.allclose(xc, xf[:, ::2, ::2, ::2], rtol=0, atol=1e-12 * float(xf.abs().max()))
+    assert uc.shape == (3, 16, 16, 9)
+
+
+def test_les_rhs_and_closure_smoke(h3):
+    """LESRHS without a closure is the Navier-Stokes RHS; with an (untrained)
+    closure it adds a finite, dealiased, divergence-free SGS force."""
+    les = importlib.import_module("3dhit_b200.les")
+    closure = importlib.import_module("3dhit_b200.closure")
+    g = h3.make_grid(32)
+    u = h3.hit_initial_field(0, g)
+    p = h3.NSParams(nu=0.01, forcing=h3.LinearForcing(0.1))
+    base = h3.make_ns_rhs(g)(u, p, 0.0)
+    assert torch.equal(les.LESRHS(g)(u, p, 0.0), base)
+    m = closure.ClosureMLP("cuda", seed=1)
+    du = les.LESRHS(g, m)(u, p, 0.0)
+    f = du - base
+    assert torch.isfinite(f).all() and float(f.abs().max()) > 0
+    assert torch.equal(f, h3.dealias(f, g))
+    div = g.kx * f[0] + g.ky * f[1] + g.kz * f[2]
+    assert float(div.abs().max()) <= 1e-4 * float(f.abs().max()) * float(g.k2.max()) ** 0.5
