@@ -48,6 +48,7 @@ class ClosureMLP:
         self.W4, self.b4 = lin(HIDDEN, OUTPUTS)
         self.x_scale = torch.ones(FEATURES, device=self.device)
         self.y_scale = torch.ones(OUTPUTS, device=self.device)
+        self.sgs_scale = 1.0  # calibration of the physical stress (energy-transfer matching)
         self._err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._ws = None
         self._packed = None
@@ -59,13 +60,17 @@ class ClosureMLP:
 
     def state_dict(self):
         d = {k: getattr(self, k).detach().cpu() for k in ("W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4")}
-        d.update(x_scale=self.x_scale.cpu(), y_scale=self.y_scale.cpu())
+        d.update(x_scale=self.x_scale.cpu(), y_scale=self.y_scale.cpu(), sgs_scale=torch.tensor(float(self.sgs_scale)))
         return d
 
     def load_state_dict(self, d):
         for k, v in d.items():
-            getattr(self, k).copy_(v.to(self.device))
+            if k == "sgs_scale":
+                self.sgs_scale = float(v)
+            else:
+                getattr(self, k).copy_(v.to(self.device))
         self._packed = None
+        self._physical = None
 
     def pack(self):
         """bf16 device operands of the kernels (rebuilt after every update)."""
@@ -111,8 +116,9 @@ class ClosureMLP:
         y_scale into W4 and b4): the network maps physical gradients to the
         physical stress."""
         W1, W4, b4 = self.W1, self.W4, self.b4
+        ys = self.y_scale * float(self.sgs_scale)
         self.W1 = W1 / self.x_scale[:, None]
-        self.W4, self.b4 = W4 * self.y_scale[None, :], b4 * self.y_scale
+        self.W4, self.b4 = W4 * ys[None, :], b4 * ys
         try:
             w = self.pack()
         finally:

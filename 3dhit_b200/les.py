@@ -154,10 +154,23 @@ def make_dataset(fine_n=256, coarse_n=64, nu=1.5e-3, E_target=1.5, spinup=2000, 
                 u0_coarse=u0_coarse, fine=fine, coarse=coarse, wall_s=time.perf_counter() - t0)
 
 
+def sgs_transfer(grads, tau):
+    """Mean SGS energy transfer -<tau_ij S_ij> (S the resolved strain rate)
+    of gradient fields (..., 9, P) and stress fields (..., 6, P)."""
+    g = grads
+    S = [g[..., 0, :], g[..., 4, :], g[..., 8, :], 0.5 * (g[..., 1, :] + g[..., 3, :]),
+         0.5 * (g[..., 2, :] + g[..., 6, :]), 0.5 * (g[..., 5, :] + g[..., 7, :])]
+    w = (1.0, 1.0, 1.0, 2.0, 2.0, 2.0)
+    return -float(sum(w[c] * (tau[..., c, :].double() * S[c].double()).mean() for c in range(6)))
+
+
 def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20, log=None):
     """Fit the closure on (X, Y) with Adam on the tensor-core gradients; the
-    last ``val_snapshots`` snapshots are held out.  Returns the model and the
-    loss history (train, validation)."""
+    last ``val_snapshots`` snapshots are held out.  The fitted stress is then
+    rescaled so that its mean SGS energy transfer -<tau_ij S_ij> over the
+    training snapshots equals the DNS's (an MSE fit shrinks the stress towards
+    zero and under-dissipates in the LES).  Returns the model and the loss
+    history (train, validation)."""
     X, Y = data["X"], data["Y"]
     S = X.shape[0]
     ntr = S - val_snapshots
@@ -192,18 +205,33 @@ def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20
             if log:
                 log(f"step {it}: train {hist[-1][1]:.4f} val {vl:.4f}")
     m.check_errors()
+    # energy-transfer calibration on the training snapshots
+    pi_true, pi_model = 0.0, 0.0
+    m.sgs_scale = 1.0
+    m.pack_physical()
+    out = torch.empty_like(Y[0])
+    for s in range(ntr):
+        m.forward_fields(X[s], out)
+        pi_true += sgs_transfer(X[s], Y[s])
+        pi_model += sgs_transfer(X[s], out)
+    m.sgs_scale = pi_true / pi_model if pi_model > 0 else 1.0
+    m._physical = None
+    hist.append(("energy_transfer_true_model_scale", pi_true / ntr, pi_model / ntr, m.sgs_scale))
+    if log:
+        log(f"SGS transfer: DNS {pi_true / ntr:.4g}, fit {pi_model / ntr:.4g}, scale {m.sgs_scale:.3f}")
     return m, hist
 
 
-def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True):
-    """Coarse LES from the first filtered snapshot's state, Lundgren forcing at
-    the DNS's mean coefficient; returns the time-averaged spectrum over the
-    samples after ``discard`` steps, the step time and the energy history."""
+def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5):
+    """Coarse LES from the first filtered snapshot's state with the DNS's
+    Lundgren forcing holding the resolved energy at the filtered DNS's mean
+    (relaxation time ``tau_relax``); returns the time-averaged spectrum over
+    the samples after ``discard`` steps, the step time and the energy
+    history."""
     coarse = data["coarse"]
-    dev = coarse.device
     kc = coarse.Nx // 3
-    A = sum(data["A"]) / len(data["A"])
-    p = NSParams(nu=data["nu"], forcing=LinearForcing(A))
+    E_res = float(data["spectra"].sum(1).mean())
+    p = NSParams(nu=data["nu"], forcing=HoldEnergyForcing(E_res, data["nu"], tau=tau_relax))
     rhs = LESRHS(coarse, closure)
     u = data["u0_coarse"].clone()
     dt = data.get("dt_les") or cfl_dt(u, coarse, 0.5)

@@ -304,7 +304,7 @@ def run_closure(args):
     """Learned SGS closure (Lundgren hold-energy forced DNS on F^3, sharp
     spectral filter to C^3 at k_c = C/3, MLP 9 -> 64x3 -> 6 on the tensor
     cores, then C^3 LES from the first filtered snapshot with Lundgren forcing
-    at the DNS's mean coefficient, with and without the closure).  Prints one
+    holding the filtered DNS's resolved energy, with and without the closure).  Prints one
     JSON line: E(k) errors against the time-averaged filtered DNS spectrum for
     k <= k_c, and the wall-time ratio of the DNS to the LES over the same
     physical time."""
@@ -338,7 +338,8 @@ def run_closure(args):
             "config": {"workload": f"Lundgren hold-E DNS {args.cl_fine}^3 (nu=1.5e-3, E_t=1.5, CFL 0.5), "
                                    f"{args.cl_spinup} spin-up steps, {args.cl_snapshots} snapshots every "
                                    f"{args.cl_every} steps, filter k_c={kc}; MLP 9->64->64->64->6 GELU bf16; "
-                                   f"LES {args.cl_les_steps} steps, Lundgren forcing at the DNS mean A"},
+                                   f"LES {args.cl_les_steps} steps, Lundgren forcing holding the filtered DNS energy "
+                                   f"(relaxation 0.5); closure rescaled to the DNS SGS energy transfer"},
             "dns_ms_per_step": data["dns_ms_per_step"], "dns_dt": data["dt"], "mean_A": sum(data["A"]) / len(data["A"]),
             "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train},
             "no_closure": out["no_closure"], "closure": out["closure"]}
