@@ -26,7 +26,7 @@ import torch
 
 from . import _native as nat
 from .closure import ClosureMLP
-from .diagnostics import energy_spectrum, energy_budget
+from .diagnostics import energy, energy_budget, energy_spectrum
 from .fields import cfl_dt, hit_initial_field
 from .forcing import HoldEnergyForcing, LinearForcing
 from .grid import _check_state, make_grid, to_physical, to_spectral
@@ -83,25 +83,33 @@ def sgs_stress(u_hat_fine, fine, coarse):
 
 
 class LESRHS:
-    """Coarse RHS with an optional learned closure (``ClosureMLP``)."""
+    """Coarse RHS with an optional learned closure (``ClosureMLP``).  With
+    ``freeze_every`` = k the SGS stress is evaluated at every k-th call (the
+    first stage of an RK4 step when k = 4) and reused in between."""
 
-    def __init__(self, grid, closure=None):
+    def __init__(self, grid, closure=None, freeze_every=1):
         self.grid = grid
         self.ns = make_ns_rhs(grid)
         self.closure = closure
+        self.freeze_every = int(freeze_every)
         self._tau = None
+        self._tau_hat = None
+        self._calls = 0
 
     def __call__(self, u_hat, params, t):
         g = self.grid
         du = self.ns(u_hat, params, t, assume_dealiased=True)
         if self.closure is not None:
-            P = g.Nx * g.Ny * g.Nz
-            grads = velocity_gradients(u_hat, g)
-            if self._tau is None:
-                self._tau = torch.empty(6, P, dtype=g.dtype, device=g.device)
-            self.closure.forward_fields(grads, self._tau)
-            tau_hat = to_spectral(self._tau.reshape(6, g.Nx, g.Ny, g.Nz), g)
-            nat.call("hit_add_sgs_force", g.plan.handle, nat.ptr(tau_hat), nat.ptr(du), nat.stream_ptr(g.device))
+            if self._calls % self.freeze_every == 0:
+                P = g.Nx * g.Ny * g.Nz
+                grads = velocity_gradients(u_hat, g)
+                if self._tau is None:
+                    self._tau = torch.empty(6, P, dtype=g.dtype, device=g.device)
+                self.closure.forward_fields(grads, self._tau)
+                self._tau_hat = to_spectral(self._tau.reshape(6, g.Nx, g.Ny, g.Nz), g)
+            self._calls += 1
+            nat.call("hit_add_sgs_force", g.plan.handle, nat.ptr(self._tau_hat), nat.ptr(du),
+                     nat.stream_ptr(g.device))
         return du
 
 
@@ -129,7 +137,7 @@ def make_dataset(fine_n=256, coarse_n=64, nu=1.5e-3, E_target=1.5, spinup=2000, 
     Pc = coarse.Nx * coarse.Ny * coarse.Nz
     X = torch.empty(snapshots, 9, Pc, device=device)
     Y = torch.empty(snapshots, 6, Pc, device=device)
-    spectra, A = [], []
+    spectra, A, E_f = [], [], []
     u0_coarse = None
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dns_ms = 0.0
@@ -146,11 +154,13 @@ def make_dataset(fine_n=256, coarse_n=64, nu=1.5e-3, E_target=1.5, spinup=2000, 
         X[s] = velocity_gradients(ub, coarse)
         Y[s] = sgs_stress(u, fine, coarse)
         spectra.append(_spectrum(ub, coarse, kc))
+        E_f.append(float(energy(ub, coarse)))
         b = energy_budget(u, fine, nu, forcing)
         A.append(float(b["eps"]) / (2.0 * float(b["E"])))  # hold-energy A = 2 nu Omega / 2E
         if log and s % 20 == 0:
             log(f"snapshot {s}: E={float(b['E']):.4f}")
-    return dict(X=X, Y=Y, spectra=torch.stack(spectra), A=A, dt=dt, nu=nu, dns_ms_per_step=dns_ms / (snapshots * every),
+    return dict(X=X, Y=Y, spectra=torch.stack(spectra), A=A, E_filtered=E_f, dt=dt, nu=nu,
+                dns_ms_per_step=dns_ms / (snapshots * every),
                 u0_coarse=u0_coarse, fine=fine, coarse=coarse, wall_s=time.perf_counter() - t0)
 
 
@@ -222,17 +232,18 @@ def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20
     return m, hist
 
 
-def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5):
+def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5, freeze_every=4):
     """Coarse LES from the first filtered snapshot's state with the DNS's
-    Lundgren forcing holding the resolved energy at the filtered DNS's mean
-    (relaxation time ``tau_relax``); returns the time-averaged spectrum over
-    the samples after ``discard`` steps, the step time and the energy
-    history."""
+    Lundgren forcing holding the total energy of the filtered DNS field (its
+    mean over the snapshots; relaxation time ``tau_relax``), the SGS stress
+    evaluated once per RK4 step (``freeze_every`` = 4); returns the
+    time-averaged spectrum over the samples after ``discard`` steps, the step
+    time and the energy history."""
     coarse = data["coarse"]
     kc = coarse.Nx // 3
-    E_res = float(data["spectra"].sum(1).mean())
+    E_res = sum(data["E_filtered"]) / len(data["E_filtered"])
     p = NSParams(nu=data["nu"], forcing=HoldEnergyForcing(E_res, data["nu"], tau=tau_relax))
-    rhs = LESRHS(coarse, closure)
+    rhs = LESRHS(coarse, closure, freeze_every=freeze_every)
     u = data["u0_coarse"].clone()
     dt = data.get("dt_les") or cfl_dt(u, coarse, 0.5)
 
