@@ -220,7 +220,8 @@ __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __res
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if constexpr (DST == 0) {
-          if constexpr (std::is_invocable<ST&, int, int, V2<T>, int>::value) st(j + r * P, col, v[r], r);
+          if constexpr (std::is_invocable<ST&, int, int, V2<T>, int, int>::value) st(j + r * P, col, v[r], r, c);
+          else if constexpr (std::is_invocable<ST&, int, int, V2<T>, int>::value) st(j + r * P, col, v[r], r);
           else st(j + r * P, col, v[r]);
         } else {
           dst[ADDR::at(j, col) + ADDR::step(r * P)] = v[r];
@@ -254,8 +255,8 @@ __device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* t
 // thread's butterflies are t = threadIdx.x + c*NT (col = t % NCOLS, b = t /
 // NCOLS); ld may take a third argument r and st a fourth, the index of the
 // value within the butterfly (position b + r*N/R in the first stage, j + r*P
-// in the last), so a caller can keep a thread's inputs or outputs in
-// registers.  The caller synchronises before ld reads shared memory written by
+// in the last), and st a fifth, the thread's butterfly index c, so a caller
+// can keep a thread's inputs or outputs in registers.  The caller synchronises before ld reads shared memory written by
 // other threads and after st writes shared memory that other threads read.
 // after_stage0() (optional) runs once every thread has finished the first
 // stage, when the loader's source may be reused.

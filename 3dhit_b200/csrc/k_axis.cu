@@ -116,8 +116,14 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
 // x-inverse of u and w = i k x u for one (ky row, z tile).  comp(c, pos, col,
 // r) gives component c of the stage input at full x position pos (zero where
 // the position is not stored); r is the index of pos in the calling thread's
-// first-stage butterfly, so a caller may serve it from registers.  The six
-// transforms are unrolled (c is a compile-time index in every call).
+// first-stage butterfly, so a caller may serve it from registers.
+//
+// The x-inverse is linear and ky, kz are constant along an x column, so of
+// w = i (ky u_z - kz u_y, kz u_x - kx u_z, kx u_y - ky u_x)
+// (navierstokes.py:73-77) only the kx terms need transforms of their own:
+// five transforms (u_x, kx u_y, kx u_z, u_y, u_z) give all six fields, w being
+// formed from them at the last stage, where a thread holds the same positions
+// of every transform (one transform's outputs are kept in registers).
 template <typename T, int N, int W, int NTH, class SRC>
 __device__ __forceinline__ void p1_body(SRC&& comp, V2<T>* A, V2<T>* B, int j, int z0, const Geom& g,
                                         const KTab<T>& kt, const V2<T>* tws, V2<T>* t6, long long t_c,
@@ -125,40 +131,55 @@ __device__ __forceinline__ void p1_body(SRC&& comp, V2<T>* A, V2<T>* B, int j, i
   const int fy = full_pos(j, g.hy, g.My, g.Ny);
   const T ky = kt.ky[fy];
   V2<T>* out = t6 + (long long)j * g.Mzp + z0;
-  // w components first, while all three stage-input components are needed;
-  // then u_z, u_x, u_y as their last readers go
-  constexpr int order[6] = {3, 4, 2, 5, 0, 1};
-#pragma unroll
-  for (int qi = 0; qi < 6; ++qi) {
-    const int q = order[qi];
-    fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
-        A, B, tws,
-        [&](int pos, int col, int r) {
-          if (q < 3) return comp(q, pos, col, r);
-          const int z = z0 + col;
-          const T kx = kt.kx[pos];
-          const T kz = z < g.Nzh ? kt.kz[z] : T(0);
-          V2<T> d;
-          if (q == 3) {
-            const V2<T> u1 = comp(1, pos, col, r), u2 = comp(2, pos, col, r);
-            d.x = ky * u2.x - kz * u1.x;
-            d.y = ky * u2.y - kz * u1.y;
-          } else if (q == 4) {
-            const V2<T> u0 = comp(0, pos, col, r), u2 = comp(2, pos, col, r);
-            d.x = kz * u0.x - kx * u2.x;
-            d.y = kz * u0.y - kx * u2.y;
-          } else {
-            const V2<T> u0 = comp(0, pos, col, r), u1 = comp(1, pos, col, r);
-            d.x = kx * u1.x - ky * u0.x;
-            d.y = kx * u1.y - ky * u0.y;
-          }
-          return cmul_i(d);
-        },
-        [&](int pos, int col, V2<T> v) { out[q * t_c + (long long)pos * t_x + col] = v; });
-    // an even stage count ends reading A, which the next transform's first
-    // stage rewrites
-    if constexpr (fft_nstages(N) % 2 == 0) __syncthreads();
-  }
+  constexpr int NS = fft_nstages(N), RL = fft_radix(N, NS - 1);
+  constexpr int CNTL = ((N / RL) * W + NTH - 1) / NTH;  // last-stage butterflies per thread
+  V2<T> keep[CNTL][RL];
+  auto kz_of = [&](int col) {
+    const int z = z0 + col;
+    return z < g.Nzh ? kt.kz[z] : T(0);
+  };
+  auto put = [&](int q, int pos, int col, V2<T> v) { out[q * t_c + (long long)pos * t_x + col] = v; };
+  auto sync = [&]() {
+    // ping-pong: an even stage count ends reading A, which the next
+    // transform's first stage rewrites
+    if constexpr (NS % 2 == 0) __syncthreads();
+  };
+  // u_x (kept)
+  fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
+      A, B, tws, [&](int pos, int col, int r) { return comp(0, pos, col, r); },
+      [&](int pos, int col, V2<T> v, int r, int c) {
+        put(0, pos, col, v);
+        keep[c][r] = v;
+      });
+  sync();
+  // kx u_y -> w_z = i (X_y - ky u_x)
+  fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
+      A, B, tws, [&](int pos, int col, int r) { return cscale(comp(1, pos, col, r), kt.kx[pos]); },
+      [&](int pos, int col, V2<T> v, int r, int c) { put(5, pos, col, cmul_i(csub(v, cscale(keep[c][r], ky)))); });
+  sync();
+  // kx u_z -> w_y = i (kz u_x - X_z)
+  fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
+      A, B, tws, [&](int pos, int col, int r) { return cscale(comp(2, pos, col, r), kt.kx[pos]); },
+      [&](int pos, int col, V2<T> v, int r, int c) {
+        put(4, pos, col, cmul_i(csub(cscale(keep[c][r], kz_of(col)), v)));
+      });
+  sync();
+  // u_y (kept)
+  fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
+      A, B, tws, [&](int pos, int col, int r) { return comp(1, pos, col, r); },
+      [&](int pos, int col, V2<T> v, int r, int c) {
+        put(1, pos, col, v);
+        keep[c][r] = v;
+      });
+  sync();
+  // u_z -> w_x = i (ky u_z - kz u_y)
+  fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
+      A, B, tws, [&](int pos, int col, int r) { return comp(2, pos, col, r); },
+      [&](int pos, int col, V2<T> v, int r, int c) {
+        put(2, pos, col, v);
+        put(3, pos, col, cmul_i(csub(cscale(v, ky), cscale(keep[c][r], kz_of(col)))));
+      });
+  sync();
 }
 
 template <typename T, int N, int W, int NTH>
