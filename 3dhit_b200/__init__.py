@@ -52,7 +52,7 @@ from .grid import (
     to_physical,
     to_spectral,
 )
-from .integrators import evolve, rk4_step, rollout
+from .integrators import SCHEMES, evolve, ifrk4_step, rk4_step, rollout
 from .adjoint import rhs_vjp, rk4_step_vjp, rollout_autograd, rollout_vjp
 from .navierstokes import NSParams, is_dealiased, linear_operator, make_ns_rhs
 
@@ -63,7 +63,7 @@ __all__ = [
     "hit_initial_field", "cfl_dt",
     "NoForcing", "LinearForcing", "BandForcing", "HoldEnergyForcing",
     "NSParams", "make_ns_rhs", "linear_operator", "is_dealiased",
-    "rk4_step", "rollout", "evolve", "rhs_vjp", "rk4_step_vjp", "rollout_vjp", "rollout_autograd",
+    "rk4_step", "ifrk4_step", "SCHEMES", "rollout", "evolve", "rhs_vjp", "rk4_step_vjp", "rollout_vjp", "rollout_autograd",
     "State", "Callback", "Diagnostic", "FieldWriter", "save_series",
     "energy", "enstrophy", "dissipation", "energy_spectrum", "component_spectra",
     "compensated_spectrum", "dissipation_constant", "kolmogorov_scale",

@@ -32,6 +32,7 @@ HIT_FORCING_BAND = 2
 HIT_FORCING_HOLD_ENERGY = 3
 
 HIT_FLAG_ASSUME_DEALIASED = 1
+HIT_FLAG_INTEGRATING_FACTOR = 2
 HIT_NUM_KERNEL_CLASSES = 6
 KERNEL_CLASSES = ("x-inverse", "y-inverse", "z-pass", "y-forward", "x-forward+epilogue", "forcing-coef")
 

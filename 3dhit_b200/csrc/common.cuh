@@ -91,6 +91,11 @@ __device__ __forceinline__ double k2_of(double kx, double ky, double kz) {
 __device__ __forceinline__ float inv_k2_of(float k2) { return k2 == 0.f ? 0.f : __frcp_rn(k2); }
 __device__ __forceinline__ double inv_k2_of(double k2) { return k2 == 0.0 ? 0.0 : __drcp_rn(k2); }
 
+// Integrating factor e^{-nu k^2 h} of the viscous operator -nu k^2
+// (navierstokes.py:100-103) over a step h, in the run precision.
+__device__ __forceinline__ float visc_factor(float nuh, float k2) { return expf(-nuh * k2); }
+__device__ __forceinline__ double visc_factor(double nuh, double k2) { return exp(-nuh * k2); }
+
 // Wavenumber tables (device): kx[Nx], ky[Ny], kz[Nzh], each value computed on the
 // host as (T)(2*pi/L * n) in double, matching grid.py:101-107.
 template <typename T> struct KTab {

@@ -292,7 +292,55 @@ __device__ __forceinline__ void p3_point(const P3Args<T>& a, int pos, int fy, in
   V2<T>* __restrict__ pacc = a.acc;
   V2<T>* __restrict__ ps = a.s;
   V2<T>* __restrict__ pout = a.out;
-  switch (a.stage) {
+  if (a.ifrk && a.stage > 0) {
+    // integrating-factor (Lawson) RK4 with E = e^{-nu k^2 dt/2} and N the RHS
+    // without its viscous term:
+    //   s2 = E (u + dt/2 k1),  s3 = E u + dt/2 k2,  s4 = E^2 u + dt E k3,
+    //   u' = E^2 u + dt/6 ((E (E k1 + 2 k2) + 2 E k3) + k4)
+    // (acc holds E k1, then E (E k1 + 2 k2), then + 2 E k3)
+    const T E = visc_factor(a.nuh, k2);
+    switch (a.stage) {
+      case 1:
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          pacc[c * a.c_c + o] = cscale(du[c], E);
+          ns[c] = cscale(cadd(us[c], cscale(du[c], a.a_next)), E);
+          ps[c * a.c_c + o] = ns[c];
+        }
+        break;
+      case 2:
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          V2<T> acn = ac[c];
+          acn.x = acn.x + T(2) * du[c].x;
+          acn.y = acn.y + T(2) * du[c].y;
+          pacc[c * a.c_c + o] = cscale(acn, E);
+          ns[c] = cadd(cscale(uu[c], E), cscale(du[c], a.a_next));
+          ps[c * a.c_c + o] = ns[c];
+        }
+        break;
+      case 3:
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const V2<T> ek = cscale(du[c], E);
+          V2<T> acn = ac[c];
+          acn.x = acn.x + T(2) * ek.x;
+          acn.y = acn.y + T(2) * ek.y;
+          pacc[c * a.c_c + o] = acn;
+          ns[c] = cadd(cscale(uu[c], E * E), cscale(ek, a.a_next));
+          ps[c * a.c_c + o] = ns[c];
+        }
+        break;
+      default:
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const V2<T> acn = cadd(ac[c], du[c]);
+          ns[c] = cadd(cscale(uu[c], E * E), cscale(acn, a.dt6));
+          pu[c * a.c_c + o] = ns[c];
+        }
+        break;
+    }
+  } else switch (a.stage) {
     case 0:
 #pragma unroll
       for (int c = 0; c < 3; ++c) {

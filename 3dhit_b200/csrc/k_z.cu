@@ -52,13 +52,18 @@ __device__ __forceinline__ V2<T> c2r_pre(const V2<T>* row, int k, int H, int Mz,
 }
 
 // r2c post-processing: output bin k in [0, H] from Z (length H), Z[i] = z(i).
-template <typename T, class ZF>
+// HALVE = false returns twice the bin (for callers that fold the 1/2 into
+// their input scale).
+template <typename T, bool HALVE = true, class ZF>
 __device__ __forceinline__ V2<T> r2c_post(ZF&& z, int k, int H, const V2<T>* twz) {
   const V2<T> a = z(k == H ? 0 : k);
   V2<T> b = z(k == 0 ? 0 : H - k);
   b.y = -b.y;
-  const V2<T> E = cscale(cadd(a, b), T(0.5));
-  const V2<T> O = cmul_mi(cscale(csub(a, b), T(0.5)));
+  V2<T> E = cadd(a, b), O = cmul_mi(csub(a, b));
+  if constexpr (HALVE) {
+    E = cscale(E, T(0.5));
+    O = cscale(O, T(0.5));
+  }
   const V2<T> w = twz[k];  // e^{-2 pi i k / Nz}
   return cadd(E, cmul(w, O));
 }
@@ -151,8 +156,9 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
           if (nxt < ngroups) prefetch(nxt);
         });
 
-    // r2c of u x w (navierstokes.py:82-86), formed while loading the first stage
-    const T s2 = a.scale * a.scale;
+    // r2c of u x w (navierstokes.py:82-86), formed while loading the first
+    // stage; the post-processing's 1/2 is folded into the product's scale
+    const T s2 = T(0.5) * a.scale * a.scale;
     fft_ip<T, H, 3 * RB, NTZ, AD, false>(
         buf, tws,
         [&](int m, int col) {
@@ -173,7 +179,7 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
       if (full || row0 + lr < a.nrows) {
         V2<T>* out = a.buf + q * a.c_stride + (row0 + lr) * Mzp;
         for (int k = lane; k < Mzp; k += 32)
-          out[k] = k < Mz ? r2c_post<T>([&](int i) { return buf[AD::at(i, col)]; }, k, H, twz) : czero<T>();
+          out[k] = k < Mz ? r2c_post<T, false>([&](int i) { return buf[AD::at(i, col)]; }, k, H, twz) : czero<T>();
       }
     }
     __syncthreads();  // buf is rewritten by the next group

@@ -84,7 +84,10 @@ template <typename T> struct P3Args {
   const V2<T>* tw;
   int stage;        // 0: rhs only (u_stage = u); 1..4: RK4 stage
   int fuse_p1;
+  int ifrk;         // 1: integrating-factor RK4 stages (nu = 0 here, the
+                    //    viscous operator enters through e^{-nu k^2 dt/2})
   T nu, a_next, dt6;
+  T nuh;            // nu dt / 2 (integrating-factor RK4)
   int forcing;
   T fA, kmin2, kmax2;
   const double* coef;  // coef[0]: band c or hold-energy A (float64)

@@ -79,10 +79,10 @@ void release(Buf& b) {
 
 struct GraphKey {
   double nu, A, eps, kmin, kmax, E_target, tau, dt;
-  int forcing;
+  int forcing, ifrk;
   bool operator==(const GraphKey& o) const {
     return nu == o.nu && A == o.A && eps == o.eps && kmin == o.kmin && kmax == o.kmax && E_target == o.E_target &&
-           tau == o.tau && dt == o.dt && forcing == o.forcing;
+           tau == o.tau && dt == o.dt && forcing == o.forcing && ifrk == o.ifrk;
   }
 };
 
@@ -194,6 +194,7 @@ template <typename T> int ensure_path(hit_plan* p, int which) {
 
 struct Scalars {
   int forcing;
+  int ifrk;  // integrating-factor RK4 (HIT_FLAG_INTEGRATING_FACTOR)
   double nu, A, eps, kmin2, kmax2, E_target, tau;
 };
 
@@ -207,6 +208,7 @@ Scalars scalars_of(const hit_params* pr) {
   s.kmax2 = pr->kmax * pr->kmax;
   s.E_target = pr->E_target;
   s.tau = pr->tau;
+  s.ifrk = (pr->flags & HIT_FLAG_INTEGRATING_FACTOR) ? 1 : 0;
   return s;
 }
 
@@ -368,7 +370,9 @@ int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt
   a.tw = tw_of<T>(p);
   a.stage = stage;
   a.fuse_p1 = fuse ? 1 : 0;
-  a.nu = (T)s.nu;
+  a.ifrk = stage > 0 && s.ifrk ? 1 : 0;
+  a.nu = a.ifrk ? (T)0 : (T)s.nu;
+  a.nuh = (T)(0.5 * dt * s.nu);
   a.a_next = stage == 3 ? (T)dt : (T)(0.5 * dt);
   a.dt6 = (T)(dt / 6.0);
   a.forcing = s.forcing;
@@ -458,7 +462,7 @@ int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
   const Scalars s = scalars_of(pr);
   if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
   if (nsteps > 0) {
-    const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing};
+    const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing, s.ifrk};
     if (!P.key_valid || !(P.key == key)) {
       for (cudaGraphExec_t& ex : P.exec) {
         if (ex) cudaGraphExecDestroy(ex);
@@ -1022,6 +1026,8 @@ int hit_rk4_step_vjp(hit_plan* p, const void* u_hat, const hit_params* pr, doubl
   if (!p || !u_hat || !ct || !u_bar) return fail(HIT_E_INVALID, "NULL argument");
   int rc;
   if ((rc = check_params(pr))) return rc;
+  if (pr->flags & HIT_FLAG_INTEGRATING_FACTOR)
+    return fail(HIT_E_UNSUPPORTED, "the integrating-factor RK4 step has no transpose");
   DeviceGuard dg(p->device);
   return DISPATCH(p, vjp_entry)(p, 1, u_hat, pr, dt, 1, 1, ct, u_bar, param_ct, (cudaStream_t)stream);
 }
@@ -1034,6 +1040,8 @@ int hit_rollout_vjp(hit_plan* p, const void* u0, const hit_params* pr, double dt
   if (checkpoint_every < 1) return fail(HIT_E_INVALID, "checkpoint_every must be >= 1");
   int rc;
   if ((rc = check_params(pr))) return rc;
+  if (pr->flags & HIT_FLAG_INTEGRATING_FACTOR)
+    return fail(HIT_E_UNSUPPORTED, "the integrating-factor RK4 step has no transpose");
   DeviceGuard dg(p->device);
   const int K = (int)std::min<int64_t>(checkpoint_every, std::max<int64_t>(nsteps, 1));
   return DISPATCH(p, vjp_entry)(p, 2, u0, pr, dt, nsteps, K, ct, u0_bar, param_ct, (cudaStream_t)stream);

@@ -21,7 +21,9 @@ from .forcing import native_params
 from .grid import _check_state
 from .navierstokes import NSRHS, resolve_flags
 
-__all__ = ["rk4_step", "rollout", "evolve"]
+__all__ = ["rk4_step", "ifrk4_step", "rollout", "evolve", "SCHEMES"]
+
+SCHEMES = ("rk4", "ifrk4")
 
 
 def _as_tensor(rhs, u_hat):
@@ -37,16 +39,28 @@ def _fused(rhs, params):
     return isinstance(rhs, NSRHS) and native_params(params.nu, params.forcing) is not None
 
 
-def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None):
-    """One classic RK4 step (integrators.py:32-38)."""
+def _flags(u_hat, g, assume_dealiased, scheme):
+    if scheme not in SCHEMES:
+        raise ValueError(f"unknown scheme {scheme!r}; expected one of {SCHEMES}")
+    f = resolve_flags(u_hat, g, assume_dealiased)
+    return f | nat.HIT_FLAG_INTEGRATING_FACTOR if scheme == "ifrk4" else f
+
+
+def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None, scheme="rk4"):
+    """One classic RK4 step (integrators.py:32-38); ``scheme="ifrk4"`` takes
+    the integrating-factor step of `ifrk4_step` instead."""
     if _fused(rhs, params):
         g = rhs.grid
         u_hat = _check_state(u_hat, g)
-        p = native_params(params.nu, params.forcing, resolve_flags(u_hat, g, assume_dealiased))
+        p = native_params(params.nu, params.forcing, _flags(u_hat, g, assume_dealiased, scheme))
         out = torch.empty_like(u_hat)
         nat.call("hit_rk4_step", g.plan.handle, nat.ptr(u_hat), p, float(dt), float(t), nat.ptr(out),
                  nat.stream_ptr(g.device))
         return out
+    if scheme == "ifrk4":
+        return _ifrk4_composed(rhs, u_hat, params, dt, t)
+    if scheme != "rk4":
+        raise ValueError(f"unknown scheme {scheme!r}; expected one of {SCHEMES}")
     u_hat = _as_tensor(rhs, u_hat)
     k1 = rhs(u_hat, params, t)
     k2 = rhs(u_hat + 0.5 * dt * k1, params, t + 0.5 * dt)
@@ -55,25 +69,66 @@ def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None):
     return u_hat + (dt / 6.0) * (k1 + 2 * k2 + 2 * k3 + k4)
 
 
-def rollout(rhs, u_hat, params, dt, nsteps, t0=0.0, *, assume_dealiased=None):
-    """Advance `nsteps` RK4 steps (integrators.py:41-53)."""
+def ifrk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None):
+    """One integrating-factor (Lawson) RK4 step on the viscous operator
+    ``linear_operator(grid, params) = -nu k^2`` (navierstokes.py:100-103), the
+    scheme the reference lists as to do (integrators.py:15-16).  With
+    E = exp(-nu k^2 dt/2) and N the RHS without its viscous term:
+
+        k1 = N(u),  k2 = N(E (u + dt/2 k1)),  k3 = N(E u + dt/2 k2),
+        k4 = N(E^2 u + dt E k3),
+        u' = E^2 u + dt/6 ((E (E k1 + 2 k2) + 2 E k3) + k4).
+
+    The viscous decay is exact, so the step is not limited by nu k^2 dt; for
+    a Beltrami field (u x w = 0) it reproduces exp(-nu k^2 t) u exactly.  With
+    the package's RHS and a built-in forcing it runs in the fused kernels at
+    the cost of an RK4 step."""
+    return rk4_step(rhs, u_hat, params, dt, t, assume_dealiased=assume_dealiased, scheme="ifrk4")
+
+
+def _ifrk4_composed(rhs, u_hat, params, dt, t):
+    """`ifrk4_step` for an RHS the fused kernels cannot run (a custom forcing
+    or another callable with a ``grid``): N(v) = rhs(v) - L v."""
+    from .navierstokes import linear_operator
+    g = getattr(rhs, "grid", None)
+    if g is None:
+        raise ValueError("ifrk4 needs rhs.grid for the linear operator")
+    u_hat = _as_tensor(rhs, u_hat)
+    L = linear_operator(g, params).to(u_hat.device)
+    E = torch.exp((0.5 * dt) * L)
+
+    def N(v, tt):
+        return rhs(v, params, tt) - L * v
+
+    k1 = N(u_hat, t)
+    k2 = N(E * (u_hat + 0.5 * dt * k1), t + 0.5 * dt)
+    k3 = N(E * u_hat + 0.5 * dt * k2, t + 0.5 * dt)
+    ek3 = E * k3
+    k4 = N((E * E) * u_hat + dt * ek3, t + dt)
+    return (E * E) * u_hat + (dt / 6.0) * ((E * (E * k1 + 2 * k2) + 2 * ek3) + k4)
+
+
+def rollout(rhs, u_hat, params, dt, nsteps, t0=0.0, *, assume_dealiased=None, scheme="rk4"):
+    """Advance `nsteps` RK4 steps (integrators.py:41-53), or integrating-factor
+    RK4 steps (`ifrk4_step`) with ``scheme="ifrk4"``."""
     nsteps = int(nsteps)
     if _fused(rhs, params):
         g = rhs.grid
         u_hat = _check_state(u_hat, g)
-        p = native_params(params.nu, params.forcing, resolve_flags(u_hat, g, assume_dealiased))
+        p = native_params(params.nu, params.forcing, _flags(u_hat, g, assume_dealiased, scheme))
         out = torch.empty_like(u_hat)
         nat.call("hit_rollout", g.plan.handle, nat.ptr(u_hat), p, float(dt), nsteps, float(t0),
                  nat.ptr(out), nat.stream_ptr(g.device))
         return out
     for i in range(nsteps):
-        u_hat = rk4_step(rhs, u_hat, params, dt, t0 + i * dt)
+        u_hat = rk4_step(rhs, u_hat, params, dt, t0 + i * dt, scheme=scheme)
     return u_hat
 
 
-def evolve(rhs, u_hat, params, grid, dt, nsteps, *, t0=0.0, callbacks=(), progress=False):
+def evolve(rhs, u_hat, params, grid, dt, nsteps, *, t0=0.0, callbacks=(), progress=False, scheme="rk4"):
     """Observation driver (integrators.py:56-109): rollout segments between
-    callback firings, callbacks fired on the segment boundaries."""
+    callback firings, callbacks fired on the segment boundaries; ``scheme``
+    as in `rollout`."""
     if isinstance(progress, bool):
         print_every = max(1, nsteps // 20) if progress else 0
     else:
@@ -105,7 +160,8 @@ def evolve(rhs, u_hat, params, grid, dt, nsteps, *, t0=0.0, callbacks=(), progre
     for n in stops:
         if _fused(rhs, params) and dealiased is None:
             dealiased = bool(resolve_flags(_check_state(u_hat, grid), grid, None))
-        u_hat = rollout(rhs, u_hat, params, dt, n - prev, t0 + prev * dt, assume_dealiased=dealiased)
+        u_hat = rollout(rhs, u_hat, params, dt, n - prev, t0 + prev * dt, assume_dealiased=dealiased,
+                        scheme=scheme)
         fire(n)
         if print_every and (n % print_every == 0 or n == nsteps):
             _print_progress(n, nsteps, t0 + n * dt, wall0)

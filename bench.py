@@ -358,6 +358,8 @@ def main():
     ap.add_argument("--shape", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="anisotropic grid for small profiling cases (overrides --size)")
     ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--scheme", default="rk4", choices=["rk4", "ifrk4"],
+                    help="time stepper: classic RK4 (the reference's) or integrating-factor RK4")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--adjoint", action="store_true", help="adjoint rollout check instead of the step benchmark")
@@ -409,7 +411,7 @@ def main():
             dist.barrier()
 
     # warm-up (captures the step graph)
-    u = h3.rollout(rhs, u0, p, dt, args.warmup, assume_dealiased=True)
+    u = h3.rollout(rhs, u0, p, dt, args.warmup, assume_dealiased=True, scheme=args.scheme)
     torch.cuda.synchronize()
 
     # ---- timed region: K graph-replayed steps ------------------------------
@@ -419,7 +421,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     e0.record(stream)
-    u = h3.rollout(rhs, u, p, dt, args.steps, assume_dealiased=True)
+    u = h3.rollout(rhs, u, p, dt, args.steps, assume_dealiased=True, scheme=args.scheme)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -437,7 +439,8 @@ def main():
     msa = (ctypes.c_double * nat.HIT_NUM_KERNEL_CLASSES)()
     cnt = (ctypes.c_int * nat.HIT_NUM_KERNEL_CLASSES)()
     out = torch.empty_like(u)
-    prm = h3.forcing.native_params(NU, p.forcing, nat.HIT_FLAG_ASSUME_DEALIASED)
+    flags = nat.HIT_FLAG_ASSUME_DEALIASED | (nat.HIT_FLAG_INTEGRATING_FACTOR if args.scheme == "ifrk4" else 0)
+    prm = h3.forcing.native_params(NU, p.forcing, flags)
     nat.call("hit_profile_rollout", g.plan.handle, nat.ptr(u), prm, float(dt), args.profile_steps,
              nat.ptr(out), msa, cnt, nat.stream_ptr(dev))
     alg = kernel_alg_bytes(N) if not args.shape else {k: 0.0 for k in nat.KERNEL_CLASSES}
@@ -482,14 +485,14 @@ def main():
     if not args.no_e2e:
         host_in = u0.cpu().pin_memory()
         host_out = torch.empty_like(host_in).pin_memory()
-        h3.rollout(rhs, host_in.to(dev, non_blocking=True), p, dt, 1)
+        h3.rollout(rhs, host_in.to(dev, non_blocking=True), p, dt, 1, scheme=args.scheme)
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(stream)
         ud = host_in.to(dev, non_blocking=True)
-        ur = h3.rollout(rhs, ud, p, dt, args.steps)  # public call: path check included
+        ur = h3.rollout(rhs, ud, p, dt, args.steps, scheme=args.scheme)  # public call: path check included
         host_out.copy_(ur, non_blocking=True)
         a1.record(stream)
         torch.cuda.synchronize()
@@ -512,7 +515,8 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": N, "dt": dt, "nu": NU,
                        "l2": "inputs larger than L2 (state + workspace ~6 GB per GPU)",
-                       "parallelism": f"replicas x{world}", "path": "dealiased (2/3-box transforms)"},
+                       "parallelism": f"replicas x{world}", "path": "dealiased (2/3-box transforms)",
+                       "scheme": args.scheme},
             "grid_point_steps_per_s": value * N**3,
             "roofline": roofline, "step_roofline": step_model, "kernels": per_kernel,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps + 1,

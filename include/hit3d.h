@@ -52,6 +52,15 @@ extern "C" {
 /* Flags (hit_params.flags). */
 #define HIT_FLAG_ASSUME_DEALIASED 1u /* input is zero outside the 2/3 box: the
                                         transforms skip those modes           */
+/* hit_rk4_step / hit_rollout advance with the integrating-factor (Lawson) RK4
+ * on the viscous operator -nu k^2 (linear_operator, navierstokes.py:100-103;
+ * the scheme the reference lists as to do, integrators.py:15-16):
+ *   E = exp(-nu k^2 dt/2), N = rhs without its -nu k^2 u term,
+ *   u' = E^2 u + dt/6 (E^2 k1 + 2E k2 + 2E k3 + k4),
+ *   k1 = N(u), k2 = N(E(u + dt/2 k1)), k3 = N(E u + dt/2 k2),
+ *   k4 = N(E^2 u + dt E k3).
+ * No reference counterpart.  hit_rhs ignores it; the transposes reject it. */
+#define HIT_FLAG_INTEGRATING_FACTOR 2u
 
 typedef struct hit_plan hit_plan;
 
