@@ -261,6 +261,10 @@ __device__ __forceinline__ void p3_point(const P3Args<T>& a, int pos, int fy, in
   const T kx = __ldg(a.k.kx + pos);
   const T k2 = k2_of(kx, ky, kz);
   const T ik2 = inv_k2_of(k2);
+  if (a.fext) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], a.fext[c * a.c_c + o]);
+  }
   if (a.forcing == 1) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) du[c] = cadd(du[c], cscale(us[c], a.fA));

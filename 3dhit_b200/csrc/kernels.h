@@ -92,6 +92,8 @@ template <typename T> struct P3Args {
   T fA, kmin2, kmax2;
   const double* coef;  // coef[0]: band c or hold-energy A (float64)
   double* partial;     // per-block (3 per block) sums of the new stage input
+  const V2<T>* fext;   // optional external force (compact layout, index o like u),
+                       // added to the nonlinear term before the mask and projection
 };
 
 // Fused z pass of the RHS: per (x, y) row, c2r of 6 components, u x w,

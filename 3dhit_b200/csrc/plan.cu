@@ -79,10 +79,10 @@ void release(Buf& b) {
 
 struct GraphKey {
   double nu, A, eps, kmin, kmax, E_target, tau, dt;
-  int forcing, ifrk;
+  int forcing, ifrk, fext;
   bool operator==(const GraphKey& o) const {
     return nu == o.nu && A == o.A && eps == o.eps && kmin == o.kmin && kmax == o.kmax && E_target == o.E_target &&
-           tau == o.tau && dt == o.dt && forcing == o.forcing && ifrk == o.ifrk;
+           tau == o.tau && dt == o.dt && forcing == o.forcing && ifrk == o.ifrk && fext == o.fext;
   }
 };
 
@@ -90,6 +90,7 @@ struct Path {  // one code path: 0 = general (full layout), 1 = dealiased (2/3 b
   Geom g{};
   bool ready = false;
   Buf t6, u6, U, ACC, S, D, partial, coef;
+  Buf FEXT;  // external force held over a call (compact layout), see hit_rollout_forced
   int p3_blocks = 0, gather_blocks = 0;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};  // [0]: last step, [1]: step that prepares the next one
   GraphKey key{};
@@ -350,7 +351,7 @@ template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st, Prof*
 
 template <typename T>
 int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt, bool fuse, bool partial,
-                    cudaStream_t st) {
+                    const V2<T>* fext, cudaStream_t st) {
   const Geom& g = P.g;
   P3Args<T> a{};
   a.t3 = vp<T>(P.t6);
@@ -381,6 +382,7 @@ int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt
   a.kmax2 = (T)s.kmax2;
   a.coef = static_cast<const double*>(P.coef.p);
   a.partial = partial ? static_cast<double*>(P.partial.p) : nullptr;
+  a.fext = fext;
   HIT_CK(launch_p3<T>(a, st));
   return HIT_OK;
 }
@@ -391,13 +393,13 @@ int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt
 // fuse_next the last stage also runs the x-inverse of the new state for the
 // following step.
 template <typename T>
-int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, bool fuse_next, cudaStream_t st,
-                 Prof* pf = nullptr) {
+int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, bool fuse_next, const V2<T>* fext,
+                 cudaStream_t st, Prof* pf = nullptr) {
   int rc;
   const bool red = needs_coef(s.forcing);
   for (int stage = 1; stage <= 4; ++stage) {
     if ((rc = launch_p2<T>(p, P, st, pf))) return rc;
-    TIMED(pf, 4, launch_p3_stage<T>(p, P, s, stage, dt, stage < 4 || fuse_next, red, st));
+    TIMED(pf, 4, launch_p3_stage<T>(p, P, s, stage, dt, stage < 4 || fuse_next, red, fext, st));
     if (red) TIMED(pf, 5, launch_coef<T>(p, P, s, P.p3_blocks, st));
   }
   return HIT_OK;
@@ -416,7 +418,7 @@ int profile_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
   pf.st = st;
   TIMED(&pf, 0, launch_p1_of<T>(p, P, vp<T>(P.U), st));
   for (int64_t i = 0; i < nsteps; ++i)
-    if ((rc = enqueue_step<T>(p, P, s, dt, i + 1 < nsteps, st, &pf))) return rc;
+    if ((rc = enqueue_step<T>(p, P, s, dt, i + 1 < nsteps, nullptr, st, &pf))) return rc;
   HIT_CK(launch_scatter<T>(vp<T>(P.U), static_cast<V2<T>*>(out), P.g, st));
   HIT_CK(cudaStreamSynchronize(st));
   for (int c = 0; c < HIT_NUM_KERNEL_CLASSES; ++c) {
@@ -438,31 +440,59 @@ int check_params(const hit_params* pr) {
   return HIT_OK;
 }
 
-template <typename T> int rhs_impl(hit_plan* p, const void* u_hat, const hit_params* pr, void* du, cudaStream_t st) {
+// External force f (reference layout) gathered into the path's compact buffer
+// FEXT, which the step epilogue adds to the nonlinear term before the mask and
+// the projection (the modes outside the 2/3 box of the dealiased path are
+// dropped by the gather, which the mask would zero anyway).
+template <typename T> int gather_force(hit_plan* p, Path& P, const void* f, cudaStream_t st) {
+  int rc;
+  if ((rc = ensure(P.FEXT, (size_t)3 * P.g.Mx * P.g.My * P.g.Mzp * sizeof(V2<T>)))) return rc;
+  GatherArgs<T> a{};
+  a.ext = static_cast<const V2<T>*>(f);
+  a.cmp = vp<T>(P.FEXT);
+  a.g = P.g;
+  a.k = ktab_of<T>(p);
+  a.partial = nullptr;
+  HIT_CK(launch_gather<T>(a, P.gather_blocks, st));
+  return HIT_OK;
+}
+
+template <typename T>
+int rhs_impl(hit_plan* p, const void* u_hat, const hit_params* pr, void* du, const void* fext, cudaStream_t st) {
   int rc;
   const int which = (pr->flags & HIT_FLAG_ASSUME_DEALIASED) ? 1 : 0;
   if ((rc = ensure_path<T>(p, which))) return rc;
   Path& P = p->path[which];
   const Scalars s = scalars_of(pr);
+  if (fext && (rc = gather_force<T>(p, P, fext, st))) return rc;
   if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
   if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
   if ((rc = launch_p2<T>(p, P, st))) return rc;
-  if ((rc = launch_p3_stage<T>(p, P, s, 0, 0.0, false, false, st))) return rc;
+  if ((rc = launch_p3_stage<T>(p, P, s, 0, 0.0, false, false, fext ? vp<T>(P.FEXT) : nullptr, st))) return rc;
   HIT_CK(launch_scatter<T>(vp<T>(P.D), static_cast<V2<T>*>(du), P.g, st));
   return HIT_OK;
 }
 
 template <typename T>
 int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, void* out,
-                 cudaStream_t st) {
+                 const void* fext, cudaStream_t st) {
   int rc;
   const int which = (pr->flags & HIT_FLAG_ASSUME_DEALIASED) ? 1 : 0;
   if ((rc = ensure_path<T>(p, which))) return rc;
   Path& P = p->path[which];
   const Scalars s = scalars_of(pr);
+  if (fext && (rc = gather_force<T>(p, P, fext, st))) return rc;
   if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
-  if (nsteps > 0) {
-    const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing, s.ifrk};
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HIT_CK(cudaStreamIsCapturing(st, &cs));
+  if (nsteps > 0 && cs != cudaStreamCaptureStatusNone) {
+    // the caller is capturing `st` into its own graph: enqueue the step
+    // kernels themselves instead of launching the plan's step graphs
+    if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
+    for (int64_t i = 0; i < nsteps; ++i)
+      if ((rc = enqueue_step<T>(p, P, s, dt, i + 1 < nsteps, fext ? vp<T>(P.FEXT) : nullptr, st))) return rc;
+  } else if (nsteps > 0) {
+    const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing, s.ifrk, fext ? 1 : 0};
     if (!P.key_valid || !(P.key == key)) {
       for (cudaGraphExec_t& ex : P.exec) {
         if (ex) cudaGraphExecDestroy(ex);
@@ -471,7 +501,7 @@ int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
       P.key_valid = false;
       for (int fused = 0; fused < 2; ++fused) {
         HIT_CK(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
-        rc = enqueue_step<T>(p, P, s, dt, fused == 1, p->cap);
+        rc = enqueue_step<T>(p, P, s, dt, fused == 1, fext ? vp<T>(P.FEXT) : nullptr, p->cap);
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(p->cap, &graph);
         if (rc) {
@@ -718,11 +748,11 @@ int rk4_vjp_impl(hit_plan* p, const V2<T>* u, const hit_params* pr, double dt, c
   V2<T>* ACC = vp<T>(p->aacc);
   const T h = (T)(0.5 * dt), d = (T)dt, d3 = (T)(dt / 3.0), d6 = (T)(dt / 6.0);
   // stage inputs (integrators.py:32-38)
-  if ((rc = rhs_impl<T>(p, u, &pg, K, st))) return rc;
+  if ((rc = rhs_impl<T>(p, u, &pg, K, nullptr, st))) return rc;
   HIT_CK(launch_axpby<T>(u, T(1), K, h, S2, n, st));
-  if ((rc = rhs_impl<T>(p, S2, &pg, K, st))) return rc;
+  if ((rc = rhs_impl<T>(p, S2, &pg, K, nullptr, st))) return rc;
   HIT_CK(launch_axpby<T>(u, T(1), K, h, S3, n, st));
-  if ((rc = rhs_impl<T>(p, S3, &pg, K, st))) return rc;
+  if ((rc = rhs_impl<T>(p, S3, &pg, K, nullptr, st))) return rc;
   HIT_CK(launch_axpby<T>(u, T(1), K, d, S4, n, st));
   // transpose of u + dt/6 (k1 + 2 k2 + 2 k3 + k4), stage by stage backwards
   HIT_CK(launch_axpby<T>(ub_in, d6, nullptr, T(0), KB, n, st));
@@ -764,12 +794,12 @@ int rollout_vjp_impl(hit_plan* p, const void* u0, const hit_params* pr, double d
   }
   HIT_CK(cudaMemcpyAsync(CK, u0, bytes, cudaMemcpyDeviceToDevice, st));
   for (int64_t j = 1; j < nseg; ++j)
-    if ((rc = rollout_impl<T>(p, CK + (j - 1) * n, &pg, dt, K, CK + j * n, st))) return rc;
+    if ((rc = rollout_impl<T>(p, CK + (j - 1) * n, &pg, dt, K, CK + j * n, nullptr, st))) return rc;
   for (int64_t j = nseg - 1; j >= 0; --j) {
     const int len = (int)std::min<int64_t>(K, nsteps - j * K);
     HIT_CK(cudaMemcpyAsync(SEG, CK + j * n, bytes, cudaMemcpyDeviceToDevice, st));
     for (int i = 1; i < len; ++i)
-      if ((rc = rollout_impl<T>(p, SEG + (i - 1) * n, &pg, dt, 1, SEG + i * n, st))) return rc;
+      if ((rc = rollout_impl<T>(p, SEG + (i - 1) * n, &pg, dt, 1, SEG + i * n, nullptr, st))) return rc;
     for (int i = len - 1; i >= 0; --i)
       if ((rc = rk4_vjp_impl<T>(p, SEG + i * n, pr, dt, UB, UB, pct, st))) return rc;
   }
@@ -977,7 +1007,28 @@ int hit_rhs(hit_plan* p, const void* u_hat, const hit_params* pr, double t, void
   int rc;
   if ((rc = check_params(pr))) return rc;
   DeviceGuard dg(p->device);
-  return DISPATCH(p, rhs_impl)(p, u_hat, pr, du, (cudaStream_t)stream);
+  return DISPATCH(p, rhs_impl)(p, u_hat, pr, du, nullptr, (cudaStream_t)stream);
+}
+
+int hit_rhs_forced(hit_plan* p, const void* u_hat, const hit_params* pr, const void* f_ext, double t, void* du,
+                   void* stream) {
+  (void)t;
+  if (!p || !u_hat || !f_ext || !du) return fail(HIT_E_INVALID, "NULL argument");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, rhs_impl)(p, u_hat, pr, du, f_ext, (cudaStream_t)stream);
+}
+
+int hit_rollout_forced(hit_plan* p, const void* u_hat, const hit_params* pr, const void* f_ext, double dt,
+                       int64_t nsteps, double t0, void* out, void* stream) {
+  (void)t0;
+  if (!p || !u_hat || !f_ext || !out) return fail(HIT_E_INVALID, "NULL argument");
+  if (nsteps < 0) return fail(HIT_E_INVALID, "nsteps must be >= 0");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, nsteps, out, f_ext, (cudaStream_t)stream);
 }
 
 int hit_rk4_step(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, double t, void* out, void* stream) {
@@ -986,7 +1037,7 @@ int hit_rk4_step(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
   int rc;
   if ((rc = check_params(pr))) return rc;
   DeviceGuard dg(p->device);
-  return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, 1, out, (cudaStream_t)stream);
+  return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, 1, out, nullptr, (cudaStream_t)stream);
 }
 
 int hit_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, double t0, void* out,
@@ -997,7 +1048,7 @@ int hit_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, double dt,
   int rc;
   if ((rc = check_params(pr))) return rc;
   DeviceGuard dg(p->device);
-  return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, nsteps, out, (cudaStream_t)stream);
+  return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, nsteps, out, nullptr, (cudaStream_t)stream);
 }
 
 int hit_profile_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, void* out,

@@ -46,17 +46,31 @@ def _flags(u_hat, g, assume_dealiased, scheme):
     return f | nat.HIT_FLAG_INTEGRATING_FACTOR if scheme == "ifrk4" else f
 
 
-def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None, scheme="rk4"):
+def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None, scheme="rk4", f_ext=None):
     """One classic RK4 step (integrators.py:32-38); ``scheme="ifrk4"`` takes
-    the integrating-factor step of `ifrk4_step` instead."""
+    the integrating-factor step of `ifrk4_step` instead.  ``f_ext``: an
+    external force held over the step (see `NSRHS.__call__`)."""
     if _fused(rhs, params):
         g = rhs.grid
         u_hat = _check_state(u_hat, g)
         p = native_params(params.nu, params.forcing, _flags(u_hat, g, assume_dealiased, scheme))
         out = torch.empty_like(u_hat)
-        nat.call("hit_rk4_step", g.plan.handle, nat.ptr(u_hat), p, float(dt), float(t), nat.ptr(out),
-                 nat.stream_ptr(g.device))
+        if f_ext is not None:
+            f_ext = _check_state(f_ext, g)
+            nat.call("hit_rollout_forced", g.plan.handle, nat.ptr(u_hat), p, nat.ptr(f_ext), float(dt), 1,
+                     float(t), nat.ptr(out), nat.stream_ptr(g.device))
+        else:
+            nat.call("hit_rk4_step", g.plan.handle, nat.ptr(u_hat), p, float(dt), float(t), nat.ptr(out),
+                     nat.stream_ptr(g.device))
         return out
+    if f_ext is not None:
+        base = rhs
+        if not isinstance(base, NSRHS):
+            raise ValueError("f_ext needs the package's RHS (make_ns_rhs)")
+
+        def rhs(u, p, tt):
+            return base(u, p, tt, f_ext=f_ext)
+        rhs.grid = base.grid
     if scheme == "ifrk4":
         return _ifrk4_composed(rhs, u_hat, params, dt, t)
     if scheme != "rk4":
@@ -108,20 +122,26 @@ def _ifrk4_composed(rhs, u_hat, params, dt, t):
     return (E * E) * u_hat + (dt / 6.0) * ((E * (E * k1 + 2 * k2) + 2 * ek3) + k4)
 
 
-def rollout(rhs, u_hat, params, dt, nsteps, t0=0.0, *, assume_dealiased=None, scheme="rk4"):
+def rollout(rhs, u_hat, params, dt, nsteps, t0=0.0, *, assume_dealiased=None, scheme="rk4", f_ext=None):
     """Advance `nsteps` RK4 steps (integrators.py:41-53), or integrating-factor
-    RK4 steps (`ifrk4_step`) with ``scheme="ifrk4"``."""
+    RK4 steps (`ifrk4_step`) with ``scheme="ifrk4"``; ``f_ext``: an external
+    force held over the whole rollout."""
     nsteps = int(nsteps)
     if _fused(rhs, params):
         g = rhs.grid
         u_hat = _check_state(u_hat, g)
         p = native_params(params.nu, params.forcing, _flags(u_hat, g, assume_dealiased, scheme))
         out = torch.empty_like(u_hat)
-        nat.call("hit_rollout", g.plan.handle, nat.ptr(u_hat), p, float(dt), nsteps, float(t0),
-                 nat.ptr(out), nat.stream_ptr(g.device))
+        if f_ext is not None:
+            f_ext = _check_state(f_ext, g)
+            nat.call("hit_rollout_forced", g.plan.handle, nat.ptr(u_hat), p, nat.ptr(f_ext), float(dt), nsteps,
+                     float(t0), nat.ptr(out), nat.stream_ptr(g.device))
+        else:
+            nat.call("hit_rollout", g.plan.handle, nat.ptr(u_hat), p, float(dt), nsteps, float(t0),
+                     nat.ptr(out), nat.stream_ptr(g.device))
         return out
     for i in range(nsteps):
-        u_hat = rk4_step(rhs, u_hat, params, dt, t0 + i * dt, scheme=scheme)
+        u_hat = rk4_step(rhs, u_hat, params, dt, t0 + i * dt, scheme=scheme, f_ext=f_ext)
     return u_hat
 
 

@@ -11,6 +11,8 @@
 * ``LESRHS``: the coarse RHS, the fused Navier-Stokes RHS plus
   project(dealias(-d_j tau_ij)) of the closure's stress (``hit_add_sgs_force``);
   without a closure it is the unmodelled coarse solver.
+* ``FusedLESStep``: one LES step on the fused step kernels, the closure's
+  force held over the step (``hit_rollout_forced``).
 * ``make_dataset`` / ``train`` / ``run_les``: the closure experiment
   (filtered forced DNS -> training -> LES against filtered DNS spectra).
 
@@ -33,7 +35,8 @@ from .grid import _check_state, make_grid, to_physical, to_spectral
 from .integrators import rk4_step, rollout
 from .navierstokes import NSParams, make_ns_rhs
 
-__all__ = ["box_filter", "velocity_gradients", "sgs_stress", "LESRHS", "make_dataset", "train", "run_les"]
+__all__ = ["box_filter", "velocity_gradients", "sgs_stress", "LESRHS", "FusedLESStep", "make_dataset", "train",
+           "run_les"]
 
 _PAIRS = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
 
@@ -111,6 +114,43 @@ class LESRHS:
             nat.call("hit_add_sgs_force", g.plan.handle, nat.ptr(self._tau_hat), nat.ptr(du),
                      nat.stream_ptr(g.device))
         return du
+
+
+class FusedLESStep:
+    """One coarse-LES RK4 step on the fused step kernels: the closure's force
+    f = project(dealias(-i k_j tau_hat_ij)) from the step's initial state
+    (``hit_velocity_gradients``, the MLP, one r2c of the six stress fields,
+    ``hit_add_sgs_force``), then one fused RK4 step with f held over its four
+    stages (``hit_rollout_forced``) -- the same scheme as `LESRHS` with
+    ``freeze_every`` = 4, without the composed stage algebra.  Without a
+    closure it is the fused step of the unmodelled coarse solver.  The
+    closure's buffers are allocated at construction, so the call can be
+    captured into a CUDA graph after one warm-up call."""
+
+    def __init__(self, grid, closure, params, dt):
+        self.grid, self.closure, self.params, self.dt = grid, closure, params, float(dt)
+        self.ns = make_ns_rhs(grid)
+        P = grid.Nx * grid.Ny * grid.Nz
+        dev = grid.device
+        self._grads = torch.empty(9, P, dtype=grid.dtype, device=dev)
+        self._tau = torch.empty(6, P, dtype=grid.dtype, device=dev)
+        self._f = torch.zeros(3, grid.Nx, grid.Ny, grid.Nz // 2 + 1, dtype=grid.cdtype, device=dev)
+
+    def force(self, u_hat):
+        """The closure's force on u_hat (the buffer is reused by the next call)."""
+        g = self.grid
+        st = nat.stream_ptr(g.device)
+        nat.call("hit_velocity_gradients", g.plan.handle, nat.ptr(u_hat), nat.ptr(self._grads), st)
+        self.closure.forward_fields(self._grads, self._tau)
+        tau_hat = to_spectral(self._tau.reshape(6, g.Nx, g.Ny, g.Nz), g)
+        self._f.zero_()
+        nat.call("hit_add_sgs_force", g.plan.handle, nat.ptr(tau_hat), nat.ptr(self._f), st)
+        return self._f
+
+    def __call__(self, u_hat):
+        u_hat = _check_state(u_hat, self.grid)
+        f = self.force(u_hat) if self.closure is not None else None
+        return rk4_step(self.ns, u_hat, self.params, self.dt, 0.0, assume_dealiased=True, f_ext=f)
 
 
 def _spectrum(u_hat, grid, kmax):
@@ -232,23 +272,28 @@ def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20
     return m, hist
 
 
-def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5, freeze_every=4):
+def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5, freeze_every=4,
+            fused=True):
     """Coarse LES from the first filtered snapshot's state with the DNS's
     Lundgren forcing holding the total energy of the filtered DNS field (its
     mean over the snapshots; relaxation time ``tau_relax``), the SGS stress
-    evaluated once per RK4 step (``freeze_every`` = 4); returns the
-    time-averaged spectrum over the samples after ``discard`` steps, the step
-    time and the energy history."""
+    evaluated once per RK4 step (``freeze_every`` = 4; `FusedLESStep` when
+    ``fused``, else the composed `LESRHS` step); returns the time-averaged
+    spectrum over the samples after ``discard`` steps, the step time and the
+    energy history."""
     coarse = data["coarse"]
     kc = coarse.Nx // 3
     E_res = sum(data["E_filtered"]) / len(data["E_filtered"])
     p = NSParams(nu=data["nu"], forcing=HoldEnergyForcing(E_res, data["nu"], tau=tau_relax))
-    rhs = LESRHS(coarse, closure, freeze_every=freeze_every)
     u = data["u0_coarse"].clone()
     dt = data.get("dt_les") or cfl_dt(u, coarse, 0.5)
+    if fused and freeze_every == 4:
+        step = FusedLESStep(coarse, closure, p, dt)
+    else:
+        rhs = LESRHS(coarse, closure, freeze_every=freeze_every)
 
-    def step(x):
-        return rk4_step(rhs, x, p, dt, 0.0)
+        def step(x):
+            return rk4_step(rhs, x, p, dt, 0.0)
 
     run = step
     if graph:

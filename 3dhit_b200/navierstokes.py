@@ -59,7 +59,10 @@ class NSRHS:
     def __init__(self, grid):
         self.grid = grid
 
-    def __call__(self, u_hat, params, t, *, assume_dealiased=None):
+    def __call__(self, u_hat, params, t, *, assume_dealiased=None, f_ext=None):
+        """rhs(u_hat, params, t); ``f_ext`` (same layout as u_hat) is an
+        external force added before the mask and the projection (no
+        reference counterpart: the coarse-LES subgrid term)."""
         g = self.grid
         u_hat = _check_state(u_hat, g)
         flags = resolve_flags(u_hat, g, assume_dealiased)
@@ -68,8 +71,13 @@ class NSRHS:
         if custom:
             p = native_params(params.nu, NoForcing(), flags)
         du = torch.empty_like(u_hat)
-        nat.call("hit_rhs", g.plan.handle, nat.ptr(u_hat), p, float(t), nat.ptr(du),
-                 nat.stream_ptr(g.device))
+        if f_ext is not None:
+            f_ext = _check_state(f_ext, g)
+            nat.call("hit_rhs_forced", g.plan.handle, nat.ptr(u_hat), p, nat.ptr(f_ext), float(t), nat.ptr(du),
+                     nat.stream_ptr(g.device))
+        else:
+            nat.call("hit_rhs", g.plan.handle, nat.ptr(u_hat), p, float(t), nat.ptr(du),
+                     nat.stream_ptr(g.device))
         if custom:
             du = du + dealias_project(params.forcing.term(u_hat, g, t) + torch.zeros_like(u_hat), g)
         return du

@@ -118,12 +118,27 @@ int hit_check_dealiased(hit_plan *plan, const void *u_hat, int *flag_dev,
 int hit_rhs(hit_plan *plan, const void *u_hat, const hit_params *params,
             double t, void *du_hat, void *stream);
 
+/* rhs and rollout with an external force f_ext (reference layout, device),
+ * held constant over the call: rhs = project(dealias(u x w + forcing + f_ext))
+ * - nu k^2 u, the RHS of a coarse LES whose subgrid-stress divergence is
+ * evaluated once per step (the learned closure).  No reference counterpart:
+ * the reference's rhs (src/hit3d/navierstokes.py:62-97) has only the forcing
+ * plug-in, whose term must be a function of u_hat. */
+int hit_rhs_forced(hit_plan *plan, const void *u_hat, const hit_params *params,
+                   const void *f_ext, double t, void *du_hat, void *stream);
+int hit_rollout_forced(hit_plan *plan, const void *u_hat,
+                       const hit_params *params, const void *f_ext, double dt,
+                       int64_t nsteps, double t0, void *out, void *stream);
+
 /* rk4_step (src/hit3d/integrators.py:32-38). */
 int hit_rk4_step(hit_plan *plan, const void *u_hat, const hit_params *params,
                  double dt, double t, void *out, void *stream);
 
 /* rollout (src/hit3d/integrators.py:41-53): nsteps RK4 steps, replayed from a
- * CUDA graph of one step; no host synchronisation inside. */
+ * CUDA graph of one step; no host synchronisation inside.  When the stream is
+ * being captured by the caller (cudaStreamIsCapturing), the step kernels are
+ * enqueued themselves, so a rollout can be part of the caller's graph (the
+ * plan's buffers must exist by then: call once before capturing). */
 int hit_rollout(hit_plan *plan, const void *u_hat, const hit_params *params,
                 double dt, int64_t nsteps, double t0, void *out, void *stream);
 
