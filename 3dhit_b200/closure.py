@@ -2,7 +2,7 @@
 
 A pointwise MLP maps the 9 filtered velocity-gradient components du_i/dx_j
 at a grid point to the 6 components of the SGS stress tau_ij
-(xx, yy, zz, xy, xz, yz): 9 -> 64 -> 64 -> 64 -> 6 with GELU, bf16 weights and
+(xx, yy, zz, xy, xz, yz): 9 -> 64 -> 64 -> 64 -> 6 with GELU (tanh form), bf16 weights and
 activations, float32 accumulation.  Forward and backward run in the
 tensor-core kernels behind ``hit_mlp_forward`` / ``hit_mlp_train_grads``
 (include/hit3d.h); torch holds the float32 master weights and runs the Adam

@@ -1,11 +1,10 @@
 // Pointwise MLP of the learned subgrid-stress closure on the fifth-generation
-// tensor cores: 9 -> 64 -> 64 -> 64 -> 6, GELU (erf form) between layers, bf16
-// weights and activations, float32 accumulation in TMEM.
+// tensor cores: 9 -> 64 -> 64 -> 64 -> 6, GELU between layers, bf16 weights
+// and activations, float32 accumulation in TMEM.
 //
 // One persistent CTA of 128 threads works on 128-point tiles; thread t owns
-// point t of the tile (its TMEM lane).  The seven weight operands (the forward
-// W^T of every layer and the backward W of layers 2-4) stay in shared memory
-// in the K-major core-matrix layout (tc_common.cuh).  Per tile:
+// point t of the tile (its TMEM lane).  The weight operands stay in shared
+// memory in the K-major core-matrix layout (tc_common.cuh).  Per tile:
 //   forward   z1 = [x, 0, 1] W1 (bias in row 15), a_l = gelu(z_l),
 //             z_l = a_{l-1} W_l + b_l (l = 2, 3), y = a3 W4 + b4;
 //   training  dy = 2 (y - tau) / (P * 6) (the MSE loss), then
@@ -14,7 +13,15 @@
 // a_{l-1} (with a ones row for the bias) and the dz_l are written feature-major
 // (aT[f][p], dzT[f][p], bf16) for the weight-gradient GEMMs
 // dW_l = a_{l-1}^T dz_l, which run on the same tensor cores (k_tcgemm).
+//
+// Two instantiations: TRAIN (forward + backward: the backward weights W_2..4
+// resident too, z1..z3 kept in 256 TMEM columns, two CTAs per SM) and the
+// inference one (forward weights only, one activation buffer, every layer's
+// accumulator in the same 64 TMEM columns: about half the shared memory, so
+// more CTAs per SM hide the per-layer MMA round trip).
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "kernels.h"
 #include "tc_common.cuh"
@@ -24,9 +31,25 @@ namespace hit {
 namespace {
 constexpr int MLP_WAIT = 1 << 22;
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks and Gimpel, 2016),
+//   gelu(x) = x/2 (1 + tanh(u)),  u = sqrt(2/pi) (x + 0.044715 x^3),
+// with the hardware tanh (tanh.approx.f32, relative error about 2^-11, below
+// the bf16 rounding the activations get next), and its exact derivative
+//   gelu'(x) = (1 + t)/2 + x/2 (1 - t^2) sqrt(2/pi) (1 + 3 * 0.044715 x^2).
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float gelu(float x) {
+  const float t = tanh_hw(x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f));
+  const float h = 0.5f * x;
+  return fmaf(h, t, h);
+}
 __device__ __forceinline__ float gelu_d(float x) {
-  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float t = tanh_hw(x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f));
+  const float du = fmaf(0.10703222440890037f, x * x, 0.7978845608028654f);
+  return fmaf(0.5f * x * fmaf(-t, t, 1.f), du, 0.5f * (1.f + t));
 }
 
 // Copy a row-major bf16 matrix [R][KC] into the K-major core-matrix layout.
@@ -52,20 +75,27 @@ __device__ __forceinline__ void store_row(unsigned char* tile, int row, const fl
 }
 }  // namespace
 
-struct MlpSmem {
+template <bool TRAIN> struct MlpSmem {
   unsigned char w1t[64 * 16 * 2], w2t[64 * 64 * 2], w3t[64 * 64 * 2], w4t[16 * 64 * 2];
-  unsigned char w4[64 * 16 * 2], w3[64 * 64 * 2], w2[64 * 64 * 2];
-  unsigned char x0[128 * 16 * 2];              // a0, later dz4
-  unsigned char buf[2][128 * 64 * 2];          // activations / gradients, ping-pong
+  // backward operands (training only)
+  unsigned char w4[TRAIN ? 64 * 16 * 2 : 16], w3[TRAIN ? 64 * 64 * 2 : 16], w2[TRAIN ? 64 * 64 * 2 : 16];
+  unsigned char x0[128 * 16 * 2];                   // a0, later dz4
+  unsigned char buf[TRAIN ? 2 : 1][128 * 64 * 2];  // activations / gradients (ping-pong when training)
   float b2[64], b3[64], b4[16];
   double red[4];
   uint64_t mbar;
   uint32_t tslot;
 };
 
+template <bool TRAIN>
 __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
+  MlpSmem<TRAIN>& S = *reinterpret_cast<MlpSmem<TRAIN>*>(smem_raw);
+  // TMEM columns of the layer accumulators: z1..z3 kept for the backward when
+  // training; one 64-column accumulator reused by every layer otherwise
+  constexpr uint32_t C1 = 0, C2 = TRAIN ? 64 : 0, C3 = TRAIN ? 128 : 0, C4 = TRAIN ? 192 : 0;
+  constexpr uint32_t NCOL = TRAIN ? 256 : 64;
+  constexpr int B1 = TRAIN ? 1 : 0;  // buffer of the second layer's output
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t mb = tc::smem_u32(&S.mbar);
   // weights and biases (resident for all tiles)
@@ -73,8 +103,8 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
   load_kmajor(S.w2t, a.w2t, 64, 64);
   load_kmajor(S.w3t, a.w3t, 64, 64);
   load_kmajor(S.w4t, a.w4t, 16, 64);
-  const bool train = a.tau != nullptr;
-  if (train) {
+  constexpr bool train = TRAIN;
+  if constexpr (TRAIN) {
     load_kmajor(S.w4, a.w4, 64, 16);
     load_kmajor(S.w3, a.w3, 64, 64);
     load_kmajor(S.w2, a.w2, 64, 64);
@@ -84,7 +114,7 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
     S.b3[i] = a.b3[i];
   }
   if (tid < 16) S.b4[tid] = a.b4[tid];
-  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), 256);
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), NCOL);
   if (tid == 0) tc::mbar_init(mb, 1);
   tc::fence_async_smem();
   tc::fence_before_sync();
@@ -147,8 +177,10 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
         for (int i = 0; i < 16; ++i) put_t(a.aT0, i, p, x[i]);
       }
     }
-    mma(0, S.x0, 16, S.w1t, 16, 1, id64);
-    ld64(0, v);
+    // (a layer's accumulator columns and input buffer are rewritten only after
+    // the MMA that reads them has completed and every thread has loaded them)
+    mma(C1, S.x0, 16, S.w1t, 16, 1, id64);
+    ld64(C1, v);
 #pragma unroll
     for (int i = 0; i < 64; ++i) v[i] = gelu(v[i]);
     store_row<64>(S.buf[0], tid, v, 64);
@@ -157,18 +189,18 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
       for (int i = 0; i < 64; ++i) put_t(a.aT1, i, p, v[i]);
       put_t(a.aT1, 64, p, 1.f);
     }
-    mma(64, S.buf[0], 64, S.w2t, 64, 4, id64);
-    ld64(64, v);
+    mma(C2, S.buf[0], 64, S.w2t, 64, 4, id64);
+    ld64(C2, v);
 #pragma unroll
     for (int i = 0; i < 64; ++i) v[i] = gelu(v[i] + S.b2[i]);
-    store_row<64>(S.buf[1], tid, v, 64);
+    store_row<64>(S.buf[B1], tid, v, 64);
     if (train && in) {
 #pragma unroll 8
       for (int i = 0; i < 64; ++i) put_t(a.aT2, i, p, v[i]);
       put_t(a.aT2, 64, p, 1.f);
     }
-    mma(128, S.buf[1], 64, S.w3t, 64, 4, id64);
-    ld64(128, v);
+    mma(C3, S.buf[B1], 64, S.w3t, 64, 4, id64);
+    ld64(C3, v);
 #pragma unroll
     for (int i = 0; i < 64; ++i) v[i] = gelu(v[i] + S.b3[i]);
     store_row<64>(S.buf[0], tid, v, 64);
@@ -177,52 +209,53 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
       for (int i = 0; i < 64; ++i) put_t(a.aT3, i, p, v[i]);
       put_t(a.aT3, 64, p, 1.f);
     }
-    mma(192, S.buf[0], 64, S.w4t, 64, 4, id16);
+    mma(C4, S.buf[0], 64, S.w4t, 64, 4, id16);
     float y[16];
-    tc::tmem_ld16(lane_base + 192, y);
+    tc::tmem_ld16(lane_base + C4, y);
 #pragma unroll
     for (int i = 0; i < 6; ++i) y[i] += S.b4[i];
     if (in && a.y) {
 #pragma unroll
       for (int i = 0; i < 6; ++i) a.y[i * a.y_sf + p * a.y_sp] = y[i];
     }
-    if (!train) continue;
-    // ---- backward ----
-    float dz[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) dz[i] = 0.f;
-    if (in) {
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        const float r = y[i] - a.tau[p * 6 + i];
-        loss += (double)r * r;
-        dz[i] = 2.f * r * a.inv_count;
-      }
-    }
-    store_row<16>(S.x0, tid, dz, 16);
-    if (in) {
-#pragma unroll
-      for (int i = 0; i < 16; ++i) put_t(a.dzT4, i, p, dz[i]);
-    }
-    // dz_l from da_l (TMEM cols 192..255) and z_l (cols zcol..)
-    auto back = [&](uint32_t zcol, unsigned char* dst, __nv_bfloat16* dzT, const float* bias) {
-      float da[64], z[64];
-      ld64(192, da);
-      ld64(zcol, z);
-#pragma unroll
-      for (int i = 0; i < 64; ++i) da[i] *= gelu_d(z[i] + (bias ? bias[i] : 0.f));
-      if (dst) store_row<64>(dst, tid, da, 64);
+    if constexpr (TRAIN) {
+      // ---- backward ----
+      float dz[16];
+  #pragma unroll
+      for (int i = 0; i < 16; ++i) dz[i] = 0.f;
       if (in) {
-#pragma unroll 8
-        for (int i = 0; i < 64; ++i) put_t(dzT, i, p, da[i]);
+  #pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          const float r = y[i] - a.tau[p * 6 + i];
+          loss += (double)r * r;
+          dz[i] = 2.f * r * a.inv_count;
+        }
       }
-    };
-    mma(192, S.x0, 16, S.w4, 16, 1, id64);  // da3 = dz4 W4^T
-    back(128, S.buf[1], a.dzT3, S.b3);
-    mma(192, S.buf[1], 64, S.w3, 64, 4, id64);  // da2 = dz3 W3^T
-    back(64, S.buf[0], a.dzT2, S.b2);
-    mma(192, S.buf[0], 64, S.w2, 64, 4, id64);  // da1 = dz2 W2^T
-    back(0, nullptr, a.dzT1, nullptr);
+      store_row<16>(S.x0, tid, dz, 16);
+      if (in) {
+  #pragma unroll
+        for (int i = 0; i < 16; ++i) put_t(a.dzT4, i, p, dz[i]);
+      }
+      // dz_l from da_l (TMEM cols 192..255) and z_l (cols zcol..)
+      auto back = [&](uint32_t zcol, unsigned char* dst, __nv_bfloat16* dzT, const float* bias) {
+        float da[64], z[64];
+        ld64(192, da);
+        ld64(zcol, z);
+  #pragma unroll
+        for (int i = 0; i < 64; ++i) da[i] *= gelu_d(z[i] + (bias ? bias[i] : 0.f));
+        if (dst) store_row<64>(dst, tid, da, 64);
+        if (in) {
+  #pragma unroll 8
+          for (int i = 0; i < 64; ++i) put_t(dzT, i, p, da[i]);
+        }
+      };
+      mma(192, S.x0, 16, S.w4, 16, 1, id64);  // da3 = dz4 W4^T
+      back(128, S.buf[1], a.dzT3, S.b3);
+      mma(192, S.buf[1], 64, S.w3, 64, 4, id64);  // da2 = dz3 W3^T
+      back(64, S.buf[0], a.dzT2, S.b2);
+      mma(192, S.buf[0], 64, S.w2, 64, 4, id64);  // da1 = dz2 W2^T
+      back(0, nullptr, a.dzT1, nullptr);
+    }
   }
   if (!ok && tid == 0) atomicExch(a.err, 1);
   if (train && a.loss) {  // per-CTA partial of sum (y - tau)^2
@@ -234,19 +267,36 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (warp == 0) tc::tmem_dealloc(tmem, 256);
+  if (warp == 0) tc::tmem_dealloc(tmem, NCOL);
 }
 
-size_t mlp_smem_bytes() { return sizeof(MlpSmem); }
+size_t mlp_smem_bytes() { return sizeof(MlpSmem<true>); }
 
+// Training pass when a.tau is set, else inference.  grid <= 0: one resident
+// wave of CTAs (at most 8 per SM: 8 x 64 TMEM columns fill the SM's 512).
 cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st) {
-  static bool ready = false;
-  if (!ready) {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+  static bool ready[2] = {false, false};
+  static int wave = 0;
+  const bool train = a.tau != nullptr;
+  const int smem = train ? (int)sizeof(MlpSmem<true>) : (int)sizeof(MlpSmem<false>);
+  if (!ready[train]) {
+    cudaError_t e = train ? cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                          : cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    ready = true;
+    if (!train) {
+      int per_sm = 0, dev = 0, sms = 0;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp<false>, 128, smem)) != cudaSuccess)
+        return e;
+      if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+      if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+      wave = std::max(1, std::min(per_sm, 8)) * sms;
+    }
+    ready[train] = true;
   }
-  k_mlp<<<grid, 128, sizeof(MlpSmem), st>>>(a);
+  const long long tiles = (a.P + 127) / 128;
+  if (grid <= 0) grid = (int)std::min<long long>(tiles, train ? 2 * 148 : wave);
+  if (train) k_mlp<true><<<grid, 128, smem, st>>>(a);
+  else k_mlp<false><<<grid, 128, smem, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -69,8 +69,7 @@ int hit_mlp_forward_strided(const hit_mlp_weights* w, const float* x, int64_t x_
   a.y_sf = y_sf;
   a.y_sp = y_sp;
   a.err = err;
-  const int grid = (int)std::min<int64_t>((P + 127) / 128, MLP_GRID);
-  cudaError_t e = hit::launch_mlp(a, grid, (cudaStream_t)stream);
+  cudaError_t e = hit::launch_mlp(a, 0, (cudaStream_t)stream);  // one resident wave of inference CTAs
   return e == cudaSuccess ? HIT_OK : cuda_err(e, "mlp_forward");
 }
 

@@ -734,7 +734,7 @@ def rollout_vjp(grid, u0, params, dt, nsteps, ub, t0=0.0, checkpoint_every=None)
 
 # ---------------------------------------------------------------------------
 # Learned SGS closure MLP (no reference counterpart): 9 -> 64 -> 64 -> 64 -> 6,
-# GELU (erf form), restated with the tensor-core kernels' bf16 roundings (bf16
+# GELU (tanh form), restated with the tensor-core kernels' bf16 roundings (bf16
 # weights, inputs, hidden activations and backward gradients; float32 biases
 # and pre-activations; sums in float64), so the CUDA forward, loss and weight
 # gradients can be checked against it.
@@ -749,14 +749,18 @@ def bf16(x):
     return b.astype(np.uint32).view(np.float32).reshape(a.shape)
 
 
+_S2PI = np.sqrt(2.0 / np.pi)
+
+
 def _gelu(x):
-    from scipy.special import erf
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks and Gimpel, 2016), the kernels' activation."""
+    t = np.tanh(_S2PI * (x + 0.044715 * x ** 3))
+    return 0.5 * x * (1.0 + t)
 
 
 def _gelu_d(x):
-    from scipy.special import erf
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(_S2PI * (x + 0.044715 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * _S2PI * (1.0 + 3 * 0.044715 * x * x)
 
 
 def mlp_loss_grads(params, x, tau):
