@@ -83,6 +83,7 @@ SIGNATURES = {
     "hit_mlp_forward_strided": (_i, [_vp, _vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _vp]),
     "hit_velocity_gradients": (_i, [_vp, _vp, _vp, _vp]),
     "hit_add_sgs_force": (_i, [_vp, _vp, _vp, _vp]),
+    "hit_sgs_force": (_i, [_vp, _vp, _vp, _vp]),
     "hit_mlp_workspace_bytes": (_i64, [_i64]),
     "hit_mlp_train_grads": (_i, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hit_energy_spectrum_noalloc": (_i, [_i, _i, _i, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),

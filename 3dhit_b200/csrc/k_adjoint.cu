@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(NT) k_grad9(const V2<T>* __restrict__ u, V2<T>
 }
 
 // du += project(dealias(-1j k_j tau_ij)), tau in the order xx, yy, zz, xy, xz, yz
-template <typename T>
+template <typename T, bool ADD>
 __global__ void __launch_bounds__(NT) k_sgs_force(const V2<T>* __restrict__ t, V2<T>* __restrict__ du, Geom gm,
                                                   KTab<T> kt) {
   const long long nm = (long long)gm.Nx * gm.Ny * gm.Nzh;
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(NT) k_sgs_force(const V2<T>* __restrict__ t, V
     f[2] = cmul_mi(s2);
     proj_mask(d, f);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) du[c * nm + m] = cadd(du[c * nm + m], f[c]);
+    for (int c = 0; c < 3; ++c) du[c * nm + m] = ADD ? cadd(du[c * nm + m], f[c]) : f[c];
   }
 }
 
@@ -350,12 +350,13 @@ template <typename T> cudaError_t launch_grad9(const V2<T>* u, V2<T>* g, const G
   return cudaGetLastError();
 }
 template <typename T>
-cudaError_t launch_sgs_force(const V2<T>* t, V2<T>* du, const Geom& gm, KTab<T> kt, cudaStream_t st) {
-  k_sgs_force<T><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(t, du, gm, kt);
+cudaError_t launch_sgs_force(const V2<T>* t, V2<T>* du, const Geom& gm, KTab<T> kt, cudaStream_t st, bool add) {
+  if (add) k_sgs_force<T, true><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(t, du, gm, kt);
+  else k_sgs_force<T, false><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(t, du, gm, kt);
   return cudaGetLastError();
 }
 template cudaError_t launch_grad9<float>(const float2*, float2*, const Geom&, KTab<float>, cudaStream_t);
 template cudaError_t launch_grad9<double>(const double2*, double2*, const Geom&, KTab<double>, cudaStream_t);
-template cudaError_t launch_sgs_force<float>(const float2*, float2*, const Geom&, KTab<float>, cudaStream_t);
-template cudaError_t launch_sgs_force<double>(const double2*, double2*, const Geom&, KTab<double>, cudaStream_t);
+template cudaError_t launch_sgs_force<float>(const float2*, float2*, const Geom&, KTab<float>, cudaStream_t, bool);
+template cudaError_t launch_sgs_force<double>(const double2*, double2*, const Geom&, KTab<double>, cudaStream_t, bool);
 }  // namespace hit

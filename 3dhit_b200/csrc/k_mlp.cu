@@ -280,16 +280,31 @@ cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st) {
   const bool train = a.tau != nullptr;
   const int smem = train ? (int)sizeof(MlpSmem<true>) : (int)sizeof(MlpSmem<false>);
   if (!ready[train]) {
-    cudaError_t e = train ? cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
-                          : cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // the largest shared-memory carveout, so that the occupancy below (and the
+    // launch) can place several CTAs per SM
+    auto setup = [&](auto kernel) {
+      cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared);
+    };
+    cudaError_t e = train ? setup(k_mlp<true>) : setup(k_mlp<false>);
     if (e != cudaSuccess) return e;
     if (!train) {
-      int per_sm = 0, dev = 0, sms = 0;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp<false>, 128, smem)) != cudaSuccess)
-        return e;
+      // CTAs per SM from the SM's shared memory and registers (1 KB of
+      // shared memory per CTA is the driver's)
+      int dev = 0, sms = 0, smem_sm = 0, regs_sm = 0;
+      cudaFuncAttributes fa{};
       if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
       if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-      wave = std::max(1, std::min(per_sm, 8)) * sms;
+      if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+        return e;
+      if ((e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev)) != cudaSuccess)
+        return e;
+      if ((e = cudaFuncGetAttributes(&fa, k_mlp<false>)) != cudaSuccess) return e;
+      const int by_smem = smem_sm / (smem + 1024);
+      const int by_regs = regs_sm / (128 * ((std::max(fa.numRegs, 1) + 7) / 8 * 8));
+      wave = std::max(1, std::min(std::min(by_smem, by_regs), 8)) * sms;
     }
     ready[train] = true;
   }

@@ -1114,17 +1114,27 @@ int hit_velocity_gradients(hit_plan* p, const void* u_hat, void* grads, void* st
   return DISPATCH(p, to_physical_impl)(p, p->ax9.p, 9, grads, (cudaStream_t)stream);
 }
 
-int hit_add_sgs_force(hit_plan* p, const void* tau_hat, void* du, void* stream) {
-  if (!p || !tau_hat || !du) return fail(HIT_E_INVALID, "NULL argument");
+namespace {
+int sgs_force_entry(hit_plan* p, const void* tau_hat, void* out, void* stream, bool add) {
+  if (!p || !tau_hat || !out) return fail(HIT_E_INVALID, "NULL argument");
   DeviceGuard dg(p->device);
   const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
   cudaError_t e = p->dtype == HIT_DTYPE_F32
-                      ? launch_sgs_force<float>(static_cast<const float2*>(tau_hat), static_cast<float2*>(du), g,
-                                                ktab_of<float>(p), (cudaStream_t)stream)
-                      : launch_sgs_force<double>(static_cast<const double2*>(tau_hat), static_cast<double2*>(du), g,
-                                                 ktab_of<double>(p), (cudaStream_t)stream);
-  if (e != cudaSuccess) return cuda_fail(e, "add_sgs_force");
+                      ? launch_sgs_force<float>(static_cast<const float2*>(tau_hat), static_cast<float2*>(out), g,
+                                                ktab_of<float>(p), (cudaStream_t)stream, add)
+                      : launch_sgs_force<double>(static_cast<const double2*>(tau_hat), static_cast<double2*>(out), g,
+                                                 ktab_of<double>(p), (cudaStream_t)stream, add);
+  if (e != cudaSuccess) return cuda_fail(e, "sgs_force");
   return HIT_OK;
+}
+}  // namespace
+
+int hit_add_sgs_force(hit_plan* p, const void* tau_hat, void* du, void* stream) {
+  return sgs_force_entry(p, tau_hat, du, stream, true);
+}
+
+int hit_sgs_force(hit_plan* p, const void* tau_hat, void* f, void* stream) {
+  return sgs_force_entry(p, tau_hat, f, stream, false);
 }
 
 int hit_tc_gemm_bf16(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M, int N, int K, int* err,

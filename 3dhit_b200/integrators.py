@@ -46,15 +46,21 @@ def _flags(u_hat, g, assume_dealiased, scheme):
     return f | nat.HIT_FLAG_INTEGRATING_FACTOR if scheme == "ifrk4" else f
 
 
-def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None, scheme="rk4", f_ext=None):
+def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None, scheme="rk4", f_ext=None, out=None):
     """One classic RK4 step (integrators.py:32-38); ``scheme="ifrk4"`` takes
     the integrating-factor step of `ifrk4_step` instead.  ``f_ext``: an
-    external force held over the step (see `NSRHS.__call__`)."""
+    external force held over the step (see `NSRHS.__call__`).  ``out``: a
+    state-shaped tensor (not ``u_hat``) that receives the new state."""
+    if out is not None and out.data_ptr() == u_hat.data_ptr():
+        raise ValueError("out must not alias u_hat")
     if _fused(rhs, params):
         g = rhs.grid
         u_hat = _check_state(u_hat, g)
         p = native_params(params.nu, params.forcing, _flags(u_hat, g, assume_dealiased, scheme))
-        out = torch.empty_like(u_hat)
+        if out is None:
+            out = torch.empty_like(u_hat)
+        elif out.shape != u_hat.shape or out.dtype != u_hat.dtype or not out.is_contiguous():
+            raise ValueError("out must be a contiguous tensor of the state's shape and dtype")
         if f_ext is not None:
             f_ext = _check_state(f_ext, g)
             nat.call("hit_rollout_forced", g.plan.handle, nat.ptr(u_hat), p, nat.ptr(f_ext), float(dt), 1,
@@ -71,6 +77,9 @@ def rk4_step(rhs, u_hat, params, dt, t, *, assume_dealiased=None, scheme="rk4", 
         def rhs(u, p, tt):
             return base(u, p, tt, f_ext=f_ext)
         rhs.grid = base.grid
+    if out is not None:
+        return out.copy_(rk4_step(rhs, u_hat, params, dt, t, assume_dealiased=assume_dealiased, scheme=scheme,
+                                  f_ext=f_ext))
     if scheme == "ifrk4":
         return _ifrk4_composed(rhs, u_hat, params, dt, t)
     if scheme != "rk4":

@@ -118,39 +118,82 @@ class LESRHS:
 
 class FusedLESStep:
     """One coarse-LES RK4 step on the fused step kernels: the closure's force
-    f = project(dealias(-i k_j tau_hat_ij)) from the step's initial state
-    (``hit_velocity_gradients``, the MLP, one r2c of the six stress fields,
-    ``hit_add_sgs_force``), then one fused RK4 step with f held over its four
-    stages (``hit_rollout_forced``) -- the same scheme as `LESRHS` with
-    ``freeze_every`` = 4, without the composed stage algebra.  Without a
-    closure it is the fused step of the unmodelled coarse solver.  The
-    closure's buffers are allocated at construction, so the call can be
-    captured into a CUDA graph after one warm-up call."""
+    f = project(dealias(-i k_j tau_hat_ij)) (``hit_velocity_gradients``, the
+    MLP, one r2c of the six stress fields, ``hit_add_sgs_force``), held over
+    the four stages of one fused RK4 step (``hit_rollout_forced``).  Without a
+    closure it is the fused step of the unmodelled coarse solver.
 
-    def __init__(self, grid, closure, params, dt):
-        self.grid, self.closure, self.params, self.dt = grid, closure, params, float(dt)
+    ``lag=False``: f from the step's initial state (the scheme of `LESRHS` with
+    ``freeze_every`` = 4).  ``lag=True``: f from the previous step's initial
+    state (the first call uses its own), computed on a second stream and a
+    second plan of the same grid concurrently with the current step; the SGS
+    term, already held over the RK stages, is then lagged by one step (first
+    order in dt like the freeze itself), and at small grids, where the step
+    kernels leave most SMs idle, the closure's cost is hidden.  All buffers are
+    allocated at construction, so a call can be captured into a CUDA graph
+    after one warm-up call."""
+
+    def __init__(self, grid, closure, params, dt, lag=False):
+        self.grid, self.closure, self.params, self.dt, self.lag = grid, closure, params, float(dt), bool(lag)
         self.ns = make_ns_rhs(grid)
         P = grid.Nx * grid.Ny * grid.Nz
         dev = grid.device
         self._grads = torch.empty(9, P, dtype=grid.dtype, device=dev)
         self._tau = torch.empty(6, P, dtype=grid.dtype, device=dev)
-        self._f = torch.zeros(3, grid.Nx, grid.Ny, grid.Nz // 2 + 1, dtype=grid.cdtype, device=dev)
+        shape = (3, grid.Nx, grid.Ny, grid.Nz // 2 + 1)
+        self._f = torch.zeros(shape, dtype=grid.cdtype, device=dev)
+        if self.lag:
+            # the closure's transforms on their own plan: plans are not re-entrant
+            self._cgrid = make_grid(grid.Nx, grid.Ny, grid.Nz, Lx=grid.Lx, Ly=grid.Ly, Lz=grid.Lz,
+                                    dtype=grid.dtype, device=dev)
+            # two force buffers that swap roles every call (the step reads one,
+            # the closure writes the other): consecutive calls alternate, so a
+            # caller capturing CUDA graphs captures two (`graph_count`)
+            self._fb = [self._f, torch.zeros(shape, dtype=grid.cdtype, device=dev)]
+            self._i = 0
+            # lowest priority: the step's kernels, on the caller's stream, go first
+            lo, _ = torch.cuda.Stream.priority_range()
+            self._side = torch.cuda.Stream(device=dev, priority=lo)
+            self._primed = False
 
-    def force(self, u_hat):
-        """The closure's force on u_hat (the buffer is reused by the next call)."""
-        g = self.grid
+    def force(self, u_hat, grid=None, out=None):
+        """The closure's force on u_hat into ``out`` (default: the step's
+        buffer, reused by the next call), with ``grid``'s plan."""
+        g = grid or self.grid
+        out = self._f if out is None else out
         st = nat.stream_ptr(g.device)
         nat.call("hit_velocity_gradients", g.plan.handle, nat.ptr(u_hat), nat.ptr(self._grads), st)
         self.closure.forward_fields(self._grads, self._tau)
         tau_hat = to_spectral(self._tau.reshape(6, g.Nx, g.Ny, g.Nz), g)
-        self._f.zero_()
-        nat.call("hit_add_sgs_force", g.plan.handle, nat.ptr(tau_hat), nat.ptr(self._f), st)
-        return self._f
+        nat.call("hit_sgs_force", g.plan.handle, nat.ptr(tau_hat), nat.ptr(out), st)
+        return out
 
-    def __call__(self, u_hat):
+    def __call__(self, u_hat, out=None):
+        """The state after one step (into ``out`` when given)."""
         u_hat = _check_state(u_hat, self.grid)
-        f = self.force(u_hat) if self.closure is not None else None
-        return rk4_step(self.ns, u_hat, self.params, self.dt, 0.0, assume_dealiased=True, f_ext=f)
+        if self.closure is None:
+            return rk4_step(self.ns, u_hat, self.params, self.dt, 0.0, assume_dealiased=True, out=out)
+        if not self.lag:
+            f = self.force(u_hat)
+            return rk4_step(self.ns, u_hat, self.params, self.dt, 0.0, assume_dealiased=True, f_ext=f, out=out)
+        cur, nxt = self._fb[self._i], self._fb[1 - self._i]
+        if not self._primed:
+            self.force(u_hat, self._cgrid, cur)
+            self._primed = True
+        main = torch.cuda.current_stream(self.grid.device)
+        self._side.wait_stream(main)
+        with torch.cuda.stream(self._side):
+            self.force(u_hat, self._cgrid, nxt)
+        out = rk4_step(self.ns, u_hat, self.params, self.dt, 0.0, assume_dealiased=True, f_ext=cur, out=out)
+        main.wait_stream(self._side)
+        self._i = 1 - self._i
+        return out
+
+    @property
+    def graph_count(self):
+        """CUDA graphs a caller captures to replay this step (2 with the lag:
+        consecutive calls swap the force buffers)."""
+        return 2 if self.lag and self.closure is not None else 1
 
 
 def _spectrum(u_hat, grid, kmax):
@@ -273,12 +316,13 @@ def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20
 
 
 def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5, freeze_every=4,
-            fused=True):
+            fused=True, lag=False):
     """Coarse LES from the first filtered snapshot's state with the DNS's
     Lundgren forcing holding the total energy of the filtered DNS field (its
     mean over the snapshots; relaxation time ``tau_relax``), the SGS stress
     evaluated once per RK4 step (``freeze_every`` = 4; `FusedLESStep` when
-    ``fused``, else the composed `LESRHS` step); returns the time-averaged
+    ``fused``, else the composed `LESRHS` step; ``lag``: the fused step's
+    lagged closure); returns the time-averaged
     spectrum over the samples after ``discard`` steps, the step time and the
     energy history."""
     coarse = data["coarse"]
@@ -288,27 +332,44 @@ def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True
     u = data["u0_coarse"].clone()
     dt = data.get("dt_les") or cfl_dt(u, coarse, 0.5)
     if fused and freeze_every == 4:
-        step = FusedLESStep(coarse, closure, p, dt)
+        step = FusedLESStep(coarse, closure, p, dt, lag=lag)
     else:
         rhs = LESRHS(coarse, closure, freeze_every=freeze_every)
 
-        def step(x):
-            return rk4_step(rhs, x, p, dt, 0.0)
+        def step(x, out=None):
+            return rk4_step(rhs, x, p, dt, 0.0, out=out)
 
     run = step
     if graph:
-        static = u.clone()
-        for _ in range(3):
-            out = step(static)
+        # the graphs advance the state between two buffers (graph k reads
+        # bufs[k] and writes bufs[1-k]; with one graph the result is copied
+        # back); with the lagged closure the two graphs also swap its force
+        # buffers
+        bufs = [u.clone(), torch.empty_like(u)]
+        for _ in range(4):  # from the initial state; an even count keeps the lag's buffer parity
+            step(bufs[0], out=bufs[1])
         torch.cuda.synchronize()
-        gph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(gph):
-            out = step(static)
+        ngraph = getattr(step, "graph_count", 1)
+        _, hi = torch.cuda.Stream.priority_range()
+        cap = torch.cuda.Stream(priority=hi)  # with the lag, the step's kernels go first
+        graphs = []
+        for k in range(ngraph):
+            gph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(gph, stream=cap):
+                if ngraph == 2:
+                    step(bufs[k], out=bufs[1 - k])
+                else:
+                    bufs[0].copy_(step(bufs[0], out=bufs[1]))
+            graphs.append(gph)
+        turn = [0]
 
         def run(x):
-            static.copy_(x)
-            gph.replay()
-            return out.clone()
+            k = turn[0]
+            if x is not bufs[k]:
+                bufs[k].copy_(x)
+            graphs[k].replay()
+            turn[0] = (k + 1) % ngraph
+            return bufs[1 - k] if ngraph == 2 else bufs[0]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     spec, n, energies = torch.zeros(kc, dtype=torch.float64), 0, []
     for i in range(1, steps + 1):

@@ -322,8 +322,8 @@ def run_closure(args):
     ref = data["spectra"].mean(0)
     kc = data["coarse"].Nx // 3
     out = {}
-    for name, cl in (("no_closure", None), ("closure", model)):
-        r = les.run_les(data, cl, steps=args.cl_les_steps, discard=args.cl_les_steps // 5)
+    for name, cl, lag in (("no_closure", None, False), ("closure", model, False), ("closure_lagged", model, True)):
+        r = les.run_les(data, cl, steps=args.cl_les_steps, discard=args.cl_les_steps // 5, lag=lag)
         rel = (r["spectrum"] / ref - 1).abs()
         T = args.cl_les_steps * r["dt"]
         dns_wall = T / data["dt"] * data["dns_ms_per_step"]
@@ -343,7 +343,7 @@ def run_closure(args):
                                    f"energy transfer"},
             "dns_ms_per_step": data["dns_ms_per_step"], "dns_dt": data["dt"], "mean_A": sum(data["A"]) / len(data["A"]),
             "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train},
-            "no_closure": out["no_closure"], "closure": out["closure"]}
+            "no_closure": out["no_closure"], "closure": out["closure"], "closure_lagged": out["closure_lagged"]}
     print(json.dumps(line), flush=True)
     return 0
 

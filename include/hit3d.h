@@ -235,11 +235,14 @@ int hit_mlp_forward_strided(const hit_mlp_weights *w, const float *x,
  * grads_out (DEVICE, 9 x Nx*Ny*Nz, the plan's dtype) receives du_i/dx_j
  * (component 3i + j) at the grid points of the state u_hat;
  * hit_add_sgs_force adds project(dealias(-1j k_j tau_hat_ij)) to du_hat, tau_hat
- * holding the 6 spectral components xx, yy, zz, xy, xz, yz. */
+ * holding the 6 spectral components xx, yy, zz, xy, xz, yz; hit_sgs_force
+ * writes it to f_hat instead (every mode: zero outside the 2/3 box). */
 int hit_velocity_gradients(hit_plan *plan, const void *u_hat, void *grads_out,
                            void *stream);
 int hit_add_sgs_force(hit_plan *plan, const void *tau_hat, void *du_hat,
                       void *stream);
+int hit_sgs_force(hit_plan *plan, const void *tau_hat, void *f_hat,
+                  void *stream);
 
 /* Bytes of DEVICE workspace hit_mlp_train_grads needs for P points. */
 int64_t hit_mlp_workspace_bytes(int64_t P);

@@ -95,3 +95,25 @@ def test_fused_les_step_matches_composed_les_rhs(h3):
     assert rel_l2(_np(a), _np(b)) < 1e-5
     assert rel_l2(_np(a), _np(c)) > 1e-4  # the closure does act
     assert rel_l2(_np(les.FusedLESStep(g, None, p, dt)(u0)), _np(c)) < 1e-5
+
+
+def test_lagged_les_step_uses_the_previous_state_force(h3):
+    les = importlib.import_module("3dhit_b200.les")
+    closure_mod = importlib.import_module("3dhit_b200.closure")
+    g = h3.make_grid(32)
+    u0 = h3.hit_initial_field(4, g)
+    nu = 0.01
+    p = h3.NSParams(nu=nu, forcing=h3.HoldEnergyForcing(E_target=1.5, nu=nu, tau=0.5))
+    cl = closure_mod.ClosureMLP(g.device, seed=2)
+    cl.x_scale.fill_(5.0)
+    cl.y_scale.fill_(2.0)
+    dt = 2e-3
+    lagged = les.FusedLESStep(g, cl, p, dt, lag=True)
+    plain = les.FusedLESStep(g, cl, p, dt)
+    u1 = lagged(u0)
+    assert torch.equal(u1, plain(u0))  # the first step uses its own state's force
+    u2 = lagged(u1)
+    f0 = plain.force(u0).clone()
+    ref = h3.rk4_step(h3.make_ns_rhs(g), u1, p, dt, 0.0, assume_dealiased=True, f_ext=f0)
+    torch.cuda.synchronize()
+    assert torch.equal(u2, ref)
