@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
     const long long o = walk.o, c = walk.c;
     const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
     V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
-    const bool zc = PF || z0 + W <= a.nz;  // whole tile inside the valid columns
+    const bool zc = z0 + W <= a.nz;  // whole tile inside the valid columns
     if (PF) {
       cp_async_wait_all();
       __syncthreads();
@@ -655,10 +655,11 @@ cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, 
     constexpr int W = tile_w<T>(NN);
     const long long ntiles = (long long)nzt * no * nc;
     if ((inv ? a.Mout : a.Min) != NN) return cudaErrorInvalidValue;  // the full side is all N rows
-    // staging needs 16-byte aligned rows and whole tiles
+    // staging needs 16-byte aligned rows and whole tiles inside the source rows
+    // (which may extend past the nz valid columns: padded rows)
     const bool pf = (sizeof(V2<T>) == 16 || ((a.s_a | a.s_o | a.s_c) % 2 == 0 &&
                                               ((uintptr_t)a.src % 16) == 0)) &&
-                    a.nz % W == 0 && nzt * W == a.nz;
+                    (long long)nzt * W <= (a.src_cols > 0 ? a.src_cols : a.nz);
     static int c[4] = {0, 0, 0, 0};
     if (pf) {
       const size_t smem = axis_smem<T, NN, W, true>();

@@ -187,54 +187,83 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   cp_async_wait_all();
 }
 
-template <typename T, int H, int RB, int NTZ>
-__global__ void __launch_bounds__(NTZ) k_zc2r(ZRealArgs<T> a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  using AD = SkewAddr<skew_ld(H)>;
-  V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);
-  V2<T>* tws = buf + RB * AD::LD;
-  const V2<T>* twz = tws + tw_size<true>(H);
-  fill_z_twiddles<T, H, NTZ>(tws, a.tw);
-  const long long row0 = (long long)blockIdx.x * RB;
-  const long long c = blockIdx.y;
-  fft_ip<T, H, RB, NTZ, AD, true>(
-      buf, tws,
-      [&](int k, int lr) {
-        if (row0 + lr >= a.nrows) return czero<T>();
-        return c2r_pre<T>(a.cbuf + c * a.cc_stride + (row0 + lr) * a.Mzp, k, H, a.Mz, twz);
-      },
-      [&](int m, int lr, V2<T> v) {
-        if (row0 + lr < a.nrows)
-          reinterpret_cast<V2<T>*>(a.rbuf + c * a.rc_stride + (row0 + lr) * (2 * H))[m] = cscale(v, a.scale);
-      });
+// Plain z c2r / r2c (to_physical / to_spectral).  Persistent CTAs walk the
+// (component, RB-row group) pairs; the rows of the next group are staged with
+// cp.async while the current group is transformed (a warp per row), as in
+// k_zcross.  Staged complex rows hold Mzp entries (16-byte chunks); real rows
+// 2H values.
+template <typename T, int H> __host__ __device__ constexpr int zreal_row_slots() {
+  return z_row_cap<H>() > H ? z_row_cap<H>() : H;  // complex rows of Mzp <= z_row_cap, or real rows of H pairs
 }
 
-template <typename T, int H, int RB, int NTZ>
-__global__ void __launch_bounds__(NTZ) k_zr2c(ZRealArgs<T> a) {
+template <typename T, int H, int RB, int NTZ, bool C2R>
+__global__ void __launch_bounds__(NTZ) k_zreal(ZRealArgs<T> a, int ncomp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using AD = SkewAddr<skew_ld(H)>;
   constexpr int KC = z_row_cap<H>();
+  constexpr int RS = zreal_row_slots<T, H>();
   V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);
   V2<T>* tws = buf + RB * AD::LD;
   const V2<T>* twz = tws + tw_size<true>(H);
+  V2<T>* raw = tws + z_tw_slots<H>();  // RB staged rows of RS slots
   fill_z_twiddles<T, H, NTZ>(tws, a.tw);
-  const long long row0 = (long long)blockIdx.x * RB;
-  const long long c = blockIdx.y;
-  fft_ip<T, H, RB, NTZ, AD, false>(
-      buf, tws,
-      [&](int m, int lr) {
-        if (row0 + lr >= a.nrows) return czero<T>();
-        return reinterpret_cast<const V2<T>*>(a.rbuf + c * a.rc_stride + (row0 + lr) * (2 * H))[m];
-      },
-      [&](int k, int lr, V2<T> v) { buf[AD::at(k, lr)] = v; });
-  for (int e = threadIdx.x; e < RB * KC; e += NTZ) {
-    const int lr = e / KC, k = e % KC;
-    if (row0 + lr < a.nrows && k < a.Mzp) {
-      V2<T> v = czero<T>();
-      if (k < a.Mz) v = r2c_post<T>([&](int i) { return buf[AD::at(i, lr)]; }, k, H, twz);
-      a.cbuf[c * a.cc_stride + (row0 + lr) * a.Mzp + k] = v;
+  const long long ngroups = (a.nrows + RB - 1) / RB, total = ngroups * ncomp;
+  constexpr int VPC = 16 / sizeof(V2<T>);
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  constexpr int NWARP = NTZ / 32;
+  // row lengths in 16-byte chunks: complex rows Mzp entries, real rows H pairs
+  const int chunks = C2R ? a.Mzp / VPC : H / VPC;
+  auto prefetch = [&](long long grp) {
+    const long long r0 = (grp % ngroups) * RB, c = grp / ngroups;
+    for (int lr = warp; lr < RB; lr += NWARP) {
+      V2<T>* dst = raw + lr * RS;
+      const bool in = r0 + lr < a.nrows;
+      const V2<T>* src = C2R ? a.cbuf + c * a.cc_stride + (r0 + lr) * a.Mzp
+                             : reinterpret_cast<const V2<T>*>(a.rbuf + c * a.rc_stride + (r0 + lr) * (2 * H));
+      for (int ch = lane; ch < chunks; ch += 32) {
+        if (in) cp_async16(dst + ch * VPC, src + ch * VPC);
+        else
+          for (int i = 0; i < VPC; ++i) dst[ch * VPC + i] = czero<T>();
+      }
+    }
+    cp_async_commit();
+  };
+  long long grp = blockIdx.x;
+  if (grp < total) prefetch(grp);
+  for (; grp < total; grp += gridDim.x) {
+    const long long row0 = (grp % ngroups) * RB, c = grp / ngroups;
+    cp_async_wait_all();
+    __syncthreads();
+    const long long nxt = grp + gridDim.x;
+    if constexpr (C2R) {
+      fft_ip<T, H, RB, NTZ, AD, true>(
+          buf, tws, [&](int k, int lr) { return c2r_pre<T>(raw + lr * RS, k, H, a.Mz, twz); },
+          [&](int m, int lr, V2<T> v) {
+            if (row0 + lr < a.nrows)
+              reinterpret_cast<V2<T>*>(a.rbuf + c * a.rc_stride + (row0 + lr) * (2 * H))[m] = cscale(v, a.scale);
+          },
+          [&]() {
+            if (nxt < total) prefetch(nxt);
+          });
+    } else {
+      fft_ip<T, H, RB, NTZ, AD, false>(
+          buf, tws, [&](int m, int lr) { return raw[lr * RS + m]; },
+          [&](int k, int lr, V2<T> v) { buf[AD::at(k, lr)] = v; },
+          [&]() {
+            if (nxt < total) prefetch(nxt);
+          });
+      for (int e = threadIdx.x; e < RB * KC; e += NTZ) {
+        const int lr = e / KC, k = e % KC;
+        if (row0 + lr < a.nrows && k < a.Mzp) {
+          V2<T> v = czero<T>();
+          if (k < a.Mz) v = r2c_post<T>([&](int i) { return buf[AD::at(i, lr)]; }, k, H, twz);
+          a.cbuf[c * a.cc_stride + (row0 + lr) * a.Mzp + k] = v;
+        }
+      }
+      __syncthreads();  // buf is rewritten by the next group
     }
   }
+  cp_async_wait_all();
 }
 
 template <typename F> cudaError_t dispatch_half(int H, F&& f) {
@@ -253,7 +282,7 @@ template <typename F> cudaError_t dispatch_half(int H, F&& f) {
 }
 
 template <typename T, int H> constexpr size_t zreal_smem() {
-  return sizeof(V2<T>) * (z_rows_per_block<H>() * skew_ld(H) + z_tw_slots<H>());
+  return sizeof(V2<T>) * (z_rows_per_block<H>() * (skew_ld(H) + zreal_row_slots<T, H>()) + z_tw_slots<H>());
 }
 
 template <typename T, int HH, int RB, int NTZ, int MINB> cudaError_t launch_zcross_v(const ZCrossArgs<T>& a, cudaStream_t st) {
@@ -279,24 +308,24 @@ template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, c
   });
 }
 
-template <typename T> cudaError_t launch_zc2r(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st) {
+template <typename T, bool C2R> cudaError_t launch_zreal(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st) {
+  if (a.Mzp % 8 || ((uintptr_t)a.cbuf % 16) || ((uintptr_t)a.rbuf % 16)) return cudaErrorInvalidValue;
   return dispatch_half(H, [&](auto hh) {
     constexpr int HH = decltype(hh)::value;
-    constexpr int RB = z_rows_per_block<HH>();
-    dim3 grid((a.nrows + RB - 1) / RB, ncomp);
-    k_zc2r<T, HH, RB, z_threads<HH>()><<<grid, z_threads<HH>(), zreal_smem<T, HH>(), st>>>(a);
+    constexpr int RB = z_rows_per_block<HH>(), NTZ = z_threads<HH>();
+    if (a.Mzp > z_row_cap<HH>()) return cudaErrorInvalidValue;
+    static int cache = 0;
+    const long long work = (a.nrows + RB - 1) / RB * ncomp;
+    const int grid = resident_grid(k_zreal<T, HH, RB, NTZ, C2R>, NTZ, zreal_smem<T, HH>(), work, cache);
+    k_zreal<T, HH, RB, NTZ, C2R><<<grid, NTZ, zreal_smem<T, HH>(), st>>>(a, ncomp);
     return cudaGetLastError();
   });
 }
-
+template <typename T> cudaError_t launch_zc2r(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st) {
+  return launch_zreal<T, true>(H, a, ncomp, st);
+}
 template <typename T> cudaError_t launch_zr2c(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st) {
-  return dispatch_half(H, [&](auto hh) {
-    constexpr int HH = decltype(hh)::value;
-    constexpr int RB = z_rows_per_block<HH>();
-    dim3 grid((a.nrows + RB - 1) / RB, ncomp);
-    k_zr2c<T, HH, RB, z_threads<HH>()><<<grid, z_threads<HH>(), zreal_smem<T, HH>(), st>>>(a);
-    return cudaGetLastError();
-  });
+  return launch_zreal<T, false>(H, a, ncomp, st);
 }
 
 template <typename T> cudaError_t prepare_axis_kernels(int Nx);
@@ -315,9 +344,9 @@ template <typename T> cudaError_t prepare_fft_kernels(int Nx, int Ny, int Nz) {
     constexpr int HH = decltype(hh)::value;
     constexpr int RB = z_rows_per_block<HH>();
     constexpr int NTZ = z_threads<HH>();
-    cudaError_t r = max_smem(k_zc2r<T, HH, RB, NTZ>, (int)zreal_smem<T, HH>());
+    cudaError_t r = max_smem(k_zreal<T, HH, RB, NTZ, true>, (int)zreal_smem<T, HH>());
     if (r != cudaSuccess) return r;
-    return max_smem(k_zr2c<T, HH, RB, NTZ>, (int)zreal_smem<T, HH>());
+    return max_smem(k_zreal<T, HH, RB, NTZ, false>, (int)zreal_smem<T, HH>());
   });
 }
 

@@ -52,6 +52,7 @@ template <typename T> struct AxisArgs {
   int Min, hin, Mout, hout;
   int nz;
   const V2<T>* tw;
+  int src_cols;  // entries per source row that may be read (0: nz); staging reads whole W-column tiles
 };
 
 // P1: x-inverse of the stage input and of curl(u): 3 compact components in,

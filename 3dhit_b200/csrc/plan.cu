@@ -553,6 +553,7 @@ template <typename T> int to_physical_impl(hit_plan* p, const void* u_hat, int n
   b.Min = b.Mout = g.Ny;
   b.hin = b.hout = g.Ny / 2;
   b.nz = g.Nzh;
+  b.src_cols = g.Mzp;  // padded rows: staged whole tiles
   b.tw = tw_of<T>(p);
   HIT_CK(launch_axis<T>(g.Ny, true, b, (g.Nzh + Wy - 1) / Wy, g.Nx, nc, st));
   ZRealArgs<T> z{};
@@ -595,6 +596,7 @@ template <typename T> int to_spectral_impl(hit_plan* p, const void* u, int nc, v
   b.Min = b.Mout = g.Ny;
   b.hin = b.hout = g.Ny / 2;
   b.nz = g.Nzh;
+  b.src_cols = g.Mzp;  // padded rows: staged whole tiles
   b.tw = tw_of<T>(p);
   HIT_CK(launch_axis<T>(g.Ny, false, b, (g.Nzh + Wy - 1) / Wy, g.Nx, nc, st));
   AxisArgs<T> a{};
@@ -609,6 +611,7 @@ template <typename T> int to_spectral_impl(hit_plan* p, const void* u, int nc, v
   a.Min = a.Mout = g.Nx;
   a.hin = a.hout = g.Nx / 2;
   a.nz = g.Nzh;
+  a.src_cols = g.Mzp;  // reads the padded rows of the workspace
   a.tw = tw_of<T>(p);
   HIT_CK(launch_axis<T>(g.Nx, false, a, (g.Nzh + Wx - 1) / Wx, g.Ny, nc, st));
   return HIT_OK;
