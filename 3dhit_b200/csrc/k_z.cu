@@ -266,6 +266,37 @@ __global__ void __launch_bounds__(NTZ) k_zreal(ZRealArgs<T> a, int ncomp) {
   cp_async_wait_all();
 }
 
+// r2c with one CTA per (RB-row group, component): many small CTAs in flight
+// hide the latency of the direct row loads, which measured faster than the
+// persistent staged form for the r2c direction.
+template <typename T, int H, int RB, int NTZ>
+__global__ void __launch_bounds__(NTZ) k_zr2c(ZRealArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  using AD = SkewAddr<skew_ld(H)>;
+  constexpr int KC = z_row_cap<H>();
+  V2<T>* buf = reinterpret_cast<V2<T>*>(smem_raw);
+  V2<T>* tws = buf + RB * AD::LD;
+  const V2<T>* twz = tws + tw_size<true>(H);
+  fill_z_twiddles<T, H, NTZ>(tws, a.tw);
+  const long long row0 = (long long)blockIdx.x * RB;
+  const long long c = blockIdx.y;
+  fft_ip<T, H, RB, NTZ, AD, false>(
+      buf, tws,
+      [&](int m, int lr) {
+        if (row0 + lr >= a.nrows) return czero<T>();
+        return reinterpret_cast<const V2<T>*>(a.rbuf + c * a.rc_stride + (row0 + lr) * (2 * H))[m];
+      },
+      [&](int k, int lr, V2<T> v) { buf[AD::at(k, lr)] = v; });
+  for (int e = threadIdx.x; e < RB * KC; e += NTZ) {
+    const int lr = e / KC, k = e % KC;
+    if (row0 + lr < a.nrows && k < a.Mzp) {
+      V2<T> v = czero<T>();
+      if (k < a.Mz) v = r2c_post<T>([&](int i) { return buf[AD::at(i, lr)]; }, k, H, twz);
+      a.cbuf[c * a.cc_stride + (row0 + lr) * a.Mzp + k] = v;
+    }
+  }
+}
+
 template <typename F> cudaError_t dispatch_half(int H, F&& f) {
   switch (H) {
     case 2: return f(std::integral_constant<int, 2>{});
@@ -281,6 +312,9 @@ template <typename F> cudaError_t dispatch_half(int H, F&& f) {
   }
 }
 
+template <typename T, int H> constexpr size_t zr2c_smem() {
+  return sizeof(V2<T>) * (z_rows_per_block<H>() * skew_ld(H) + z_tw_slots<H>());
+}
 template <typename T, int H> constexpr size_t zreal_smem() {
   return sizeof(V2<T>) * (z_rows_per_block<H>() * (skew_ld(H) + zreal_row_slots<T, H>()) + z_tw_slots<H>());
 }
@@ -325,7 +359,13 @@ template <typename T> cudaError_t launch_zc2r(int H, const ZRealArgs<T>& a, int 
   return launch_zreal<T, true>(H, a, ncomp, st);
 }
 template <typename T> cudaError_t launch_zr2c(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st) {
-  return launch_zreal<T, false>(H, a, ncomp, st);
+  return dispatch_half(H, [&](auto hh) {
+    constexpr int HH = decltype(hh)::value;
+    constexpr int RB = z_rows_per_block<HH>();
+    dim3 grid((a.nrows + RB - 1) / RB, ncomp);
+    k_zr2c<T, HH, RB, z_threads<HH>()><<<grid, z_threads<HH>(), zr2c_smem<T, HH>(), st>>>(a);
+    return cudaGetLastError();
+  });
 }
 
 template <typename T> cudaError_t prepare_axis_kernels(int Nx);
@@ -346,7 +386,7 @@ template <typename T> cudaError_t prepare_fft_kernels(int Nx, int Ny, int Nz) {
     constexpr int NTZ = z_threads<HH>();
     cudaError_t r = max_smem(k_zreal<T, HH, RB, NTZ, true>, (int)zreal_smem<T, HH>());
     if (r != cudaSuccess) return r;
-    return max_smem(k_zreal<T, HH, RB, NTZ, false>, (int)zreal_smem<T, HH>());
+    return max_smem(k_zr2c<T, HH, RB, NTZ>, (int)zr2c_smem<T, HH>());
   });
 }
 
