@@ -25,9 +25,15 @@ namespace hit {
 constexpr int TWN = 2048;  // twiddle table length (supports N <= 2048)
 
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
-__host__ __device__ constexpr int fft_nstages(int N) { return (ilog2(N) + 2) / 3; }
+// Radix-8 plan of the column transforms: radix-8 stages, with one radix-4
+// first stage when log2(N) = 2 mod 3; when log2(N) = 1 mod 3 (N = 128, 1024)
+// one radix-16 second stage (8 x 16 x 8 for 1024: the first and the last stage
+// are radix 8, which the register-mode x-forward epilogue needs); N = 16 is
+// 2 x 8.
+__host__ __device__ constexpr bool fft_has16(int N) { return ilog2(N) % 3 == 1 && N >= 128; }
+__host__ __device__ constexpr int fft_nstages(int N) { return fft_has16(N) ? (ilog2(N) - 1) / 3 : (ilog2(N) + 2) / 3; }
 __host__ __device__ constexpr int fft_radix(int N, int s) {
-  return (ilog2(N) % 3 != 0 && s == 0) ? (ilog2(N) % 3 == 1 ? 2 : 4) : 8;
+  return fft_has16(N) ? (s == 1 ? 16 : 8) : ((ilog2(N) % 3 != 0 && s == 0) ? (ilog2(N) % 3 == 1 ? 2 : 4) : 8);
 }
 __host__ __device__ constexpr int fft_pprod(int N, int s) {
   return s == 0 ? 1 : fft_pprod(N, s - 1) * fft_radix(N, s - 1);

@@ -221,13 +221,13 @@ __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
   }
 }
 
-// Register-resident P3: with a uniform radix-8 plan and one butterfly per
-// thread (N/8 * W == NTH) the forward transform's last stage leaves thread
+// Register-resident P3: with radix-8 first and last stages and one butterfly
+// per thread of those (N/8 * W == NTH) the forward transform's last stage leaves thread
 // (b, col) holding positions b + r*N/8, exactly the inputs its first inverse
 // stage needs, so the nonlinear term, the epilogue and the new stage input
 // never pass through shared memory.
 template <int N, int W, int NTH> __host__ __device__ constexpr bool p3_in_regs() {
-  return N >= 64 && ilog2(N) % 3 == 0 && (N / 8) * W == NTH;
+  return N >= 64 && fft_radix(N, 0) == 8 && fft_radix(N, fft_nstages(N) - 1) == 8 && (N / 8) * W == NTH;
 }
 
 // State rows of one mode for the epilogue: us = stage input (u for stages

@@ -14,7 +14,7 @@ from conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
 
-DIMS = [(64, 64, 64), (32, 64, 128), (128, 32, 16)]
+DIMS = [(64, 64, 64), (32, 64, 128), (128, 32, 16), (16, 16, 1024), (16, 8, 4)]
 
 
 def _tol(dtype):
