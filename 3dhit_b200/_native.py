@@ -71,6 +71,7 @@ SIGNATURES = {
     "hit_rk4_step": (_i, [_vp, _vp, _PP, _d, _d, _vp, _vp]),
     "hit_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _d, _vp, _vp]),
     "hit_rhs_forced": (_i, [_vp, _vp, _PP, _vp, _d, _vp, _vp]),
+    "hit_device_status": (_i, [ctypes.POINTER(ctypes.c_int)]),
     "hit_rollout_forced": (_i, [_vp, _vp, _PP, _vp, _d, _i64, _d, _vp, _vp]),
     "hit_profile_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _vp, _vp, _vp, _vp]),
     "hit_rhs_vjp": (_i, [_vp, _vp, _PP, _d, _vp, _vp, _vp, _vp]),

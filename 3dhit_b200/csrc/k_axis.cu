@@ -20,6 +20,7 @@
 
 #include "fft_core.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 namespace hit {
 
@@ -49,54 +50,95 @@ struct TileWalk {
   }
 };
 
-// PF: the next tile's stored rows are staged in shared memory with cp.async
-// while the current tile is transformed (needs 16-byte aligned rows/columns
-// and whole tiles).  The staging buffer holds all N positions: rows that are
-// not stored stay zero from the kernel start, so the first stage reads it
+// PF (staging mode): 0 = the first stage reads global memory directly;
+// 1 = the next tile's stored rows are staged in shared memory with cp.async
+// while the current tile is transformed (16-byte aligned rows, whole tiles
+// inside the source rows); 2 = the same staging with TMA: one thread loads the
+// tile as boxes of br rows x W columns through two tensor maps, one over the
+// stored rows [0, hin) (to positions [0, ka*br)) and one over [hin, Min) (to
+// positions [N - kb*br, N), the boxes aligned to the end of that half); rows
+// of a box outside its half are zero-filled by the TMA unit and land in the
+// gap between the halves.  The staging buffer holds all N positions: rows that
+// are never loaded stay zero from the kernel start, so the first stage reads it
 // without checks.  The inverse transform always writes all N rows and the
 // forward one always reads all N rows (the launcher checks this).
-template <typename T, int N, int W, bool INV, bool PF>
-__global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int ntiles) {
+constexpr int AXIS_WAIT = 1 << 22;  // mbarrier polls before a TMA wait gives up
+__device__ int g_axis_timeout = 0;  // set when a TMA wait gave up (hit_device_status)
+
+template <typename T, int N, int W, bool INV, int PF>
+__global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int ntiles,
+                                             const __grid_constant__ CUtensorMap mapA,
+                                             const __grid_constant__ CUtensorMap mapB) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t tbar;
   V2<T>* A = reinterpret_cast<V2<T>*>(smem_raw);
   V2<T>* B = A + skew8_slots(N, W);
   V2<T>* tws = B + skew8_slots(N, W);
-  V2<T>* stg = tws + ((tw_size<false>(N) + 1) / 2 * 2);  // PF: N x W staged rows
+  // N x W staged rows, 128-byte aligned (TMA destinations)
+  V2<T>* stg = reinterpret_cast<V2<T>*>(
+      (reinterpret_cast<uintptr_t>(tws + ((tw_size<false>(N) + 1) / 2 * 2)) + 127) & ~(uintptr_t)127);
   fill_stage_twiddles<T, N, false, NT>(tws, a.tw);
   constexpr int VPC = 16 / sizeof(V2<T>);
+  constexpr int XE = sizeof(V2<T>) / 8;  // 8-byte tensor elements per complex value
+  const uint32_t mb = tma::smem_u32(&tbar);
   auto prefetch = [&](const TileWalk& w) {
-    const V2<T>* src = a.src + w.c * a.s_c + w.o * a.s_o + w.zt * W;
-    constexpr int CPR = W / VPC;  // 16-byte chunks per row
-    for (int e = threadIdx.x; e < a.Min * CPR; e += NT) {
-      const int row = e / CPR, ch = e % CPR;
-      cp_async16(stg + full_pos(row, a.hin, a.Min, N) * W + ch * VPC, src + (long long)row * a.s_a + ch * VPC);
+    if constexpr (PF == 1) {
+      const V2<T>* src = a.src + w.c * a.s_c + w.o * a.s_o + w.zt * W;
+      constexpr int CPR = W / VPC;  // 16-byte chunks per row
+      for (int e = threadIdx.x; e < a.Min * CPR; e += NT) {
+        const int row = e / CPR, ch = e % CPR;
+        cp_async16(stg + full_pos(row, a.hin, a.Min, N) * W + ch * VPC, src + (long long)row * a.s_a + ch * VPC);
+      }
+      cp_async_commit();
+    } else if constexpr (PF == 2) {
+      if (threadIdx.x == 0) {
+        tma::mbar_expect_tx(mb, (uint32_t)((a.ka + a.kb) * a.br * W * sizeof(V2<T>)));
+        const int x = w.zt * W * XE;
+        for (int k = 0; k < a.ka; ++k) tma::load4(stg + k * a.br * W, &mapA, x, k * a.br, w.o, w.c, mb);
+        for (int k = 0; k < a.kb; ++k)
+          tma::load4(stg + (N - (k + 1) * a.br) * W, &mapB, x, a.pb - (k + 1) * a.br, w.o, w.c, mb);
+      }
     }
-    cp_async_commit();
   };
-  if (PF) {
+  if constexpr (PF == 1) {
     for (int e = threadIdx.x; e < (N - a.Min) * W; e += NT) stg[a.hin * W + e] = czero<T>();
+  } else if constexpr (PF == 2) {
+    for (int e = threadIdx.x; e < (N - (a.ka + a.kb) * a.br) * W; e += NT) stg[a.ka * a.br * W + e] = czero<T>();
+    if (threadIdx.x == 0) tma::mbar_init(mb, 1);
+    tma::fence_async_smem();
   }
   TileWalk walk(blockIdx.x, gridDim.x, nzt, no);
   pdl_wait();
   pdl_trigger();
-  if (PF && blockIdx.x < ntiles) prefetch(walk);
   __syncthreads();
+  if (PF != 0 && blockIdx.x < ntiles) prefetch(walk);
+  if constexpr (PF != 2) __syncthreads();
+  uint32_t phase = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int z0 = walk.zt * W;
     const long long o = walk.o, c = walk.c;
     const V2<T>* src = a.src + c * a.s_c + o * a.s_o + z0;
     V2<T>* dst = a.dst + c * a.d_c + o * a.d_o + z0;
     const bool zc = z0 + W <= a.nz;  // whole tile inside the valid columns
-    if (PF) {
+    if constexpr (PF == 1) {
       cp_async_wait_all();
       __syncthreads();
+    } else if constexpr (PF == 2) {
+      // the tile's boxes have landed (a verdict shared by the block)
+      const bool ok = __syncthreads_and(tma::mbar_wait(mb, phase, AXIS_WAIT)) != 0;
+      phase ^= 1;
+      if (!ok) {
+        if (threadIdx.x == 0) atomicExch(&g_axis_timeout, 1);
+        tma::mbar_wait(mb, phase ^ 1, AXIS_WAIT);  // the copies in flight, once more with a limit
+        return;
+      }
     }
     const int nxt = tile + gridDim.x;
     const TileWalk nwalk = walk.next();
     fft_io<T, N, W, NT, TileAddr<N, W>, INV>(
         A, B, tws,
         [&](int pos, int col) {
-          if (PF) return stg[pos * W + col];
+          if (PF != 0) return stg[pos * W + col];
           const int row = INV ? compact_row(pos, a.hin, a.Min, N) : pos;
           return (row >= 0 && (zc || z0 + col < a.nz)) ? src[(long long)row * a.s_a + col] : czero<T>();
         },
@@ -105,12 +147,12 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
           if (row >= 0 && (zc || z0 + col < a.nz)) dst[(long long)row * a.d_a + col] = v;
         },
         [&]() {
-          if (PF && nxt < ntiles) prefetch(nwalk);
+          if (PF != 0 && nxt < ntiles) prefetch(nwalk);
         });
     __syncthreads();  // the next tile's first stage rewrites A
     walk = nwalk;
   }
-  if (PF) cp_async_wait_all();
+  if constexpr (PF == 1) cp_async_wait_all();
 }
 
 // x-inverse of u and w = i k x u for one (ky row, z tile).  comp(c, pos, col,
@@ -645,7 +687,49 @@ template <typename T, int N, int W, int NTH> size_t p3_smem(int Mx) {
   return sizeof(V2<T>) * ((size_t)2 * skew8_slots(N, W) + N * W + tw_slots_even<N>() + f);
 }
 template <typename T, int N, int W, bool PF> constexpr size_t axis_smem() {
-  return sizeof(V2<T>) * (2 * skew8_slots(N, W) + (PF ? N * W : 0) + tw_slots_even<N>());
+  // + 128 bytes: the staging tile is aligned to 128 bytes
+  return sizeof(V2<T>) * (2 * skew8_slots(N, W) + (PF ? N * W : 0) + tw_slots_even<N>()) + (PF ? 128 : 0);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to
+// the driver library).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// Tensor map over rows [row0, row0 + rows) of a (c, o, row, z) array of
+// complex values: dims (z in 8-byte elements, row, o, c), box (W columns, br
+// rows, 1, 1).  False if the layout cannot be described (the caller stages
+// with cp.async instead).
+template <typename T>
+bool axis_map(CUtensorMap* m, const V2<T>* base, long long cols, int rows, int no, int nc, long long s_a,
+              long long s_o, long long s_c, int W, int br) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc || rows < 1) return false;
+  constexpr int XE = sizeof(V2<T>) / 8;
+  const cuuint64_t dims[4] = {(cuuint64_t)(cols * XE), (cuuint64_t)rows, (cuuint64_t)no, (cuuint64_t)nc};
+  const cuuint64_t strides[3] = {(cuuint64_t)(s_a * sizeof(V2<T>)), (cuuint64_t)(s_o * sizeof(V2<T>)),
+                                 (cuuint64_t)(s_c * sizeof(V2<T>))};
+  const cuuint32_t box[4] = {(cuuint32_t)(W * XE), (cuuint32_t)br, 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, const_cast<V2<T>*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <typename T>
@@ -660,25 +744,57 @@ cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, 
     const bool pf = (sizeof(V2<T>) == 16 || ((a.s_a | a.s_o | a.s_c) % 2 == 0 &&
                                               ((uintptr_t)a.src % 16) == 0)) &&
                     (long long)nzt * W <= (a.src_cols > 0 ? a.src_cols : a.nz);
-    static int c[4] = {0, 0, 0, 0};
+    static int c[6] = {0, 0, 0, 0, 0, 0};
+    CUtensorMap mA{}, mB{};
     if (pf) {
+      // TMA staging when the layout has a tensor map: box rows br (a power of
+      // two <= 64) such that the boxes of the two halves do not overlap
+      AxisArgs<T> t = a;
+      t.pb = a.Min - a.hin;
+      t.br = 64;
+      auto nb = [](int rows, int br) { return (rows + br - 1) / br; };
+      while (t.br > 2 && t.br * (nb(a.hin, t.br) + nb(t.pb, t.br)) > NN) t.br /= 2;
+      t.ka = nb(a.hin, t.br);
+      t.kb = nb(t.pb, t.br);
+      const long long cols = a.src_cols > 0 ? a.src_cols : a.nz;
+      const bool tma = a.hin >= 1 && t.pb >= 1 && t.br * (t.ka + t.kb) <= NN && ((uintptr_t)a.src % 16) == 0 &&
+                       axis_map<T>(&mA, a.src, cols, a.hin, no, nc, a.s_a, a.s_o, a.s_c, W, t.br) &&
+                       axis_map<T>(&mB, a.src + (long long)a.hin * a.s_a, cols, t.pb, no, nc, a.s_a, a.s_o, a.s_c, W,
+                                   t.br);
       const size_t smem = axis_smem<T, NN, W, true>();
+      if (tma) {
+        if (inv)
+          return launch_pdl(k_axis<T, NN, W, true, 2>, resident_grid(k_axis<T, NN, W, true, 2>, NT, smem, ntiles, c[4]),
+                            NT, smem, st, t, nzt, no, (int)ntiles, mA, mB);
+        return launch_pdl(k_axis<T, NN, W, false, 2>, resident_grid(k_axis<T, NN, W, false, 2>, NT, smem, ntiles, c[5]),
+                          NT, smem, st, t, nzt, no, (int)ntiles, mA, mB);
+      }
       if (inv)
-        return launch_pdl(k_axis<T, NN, W, true, true>, resident_grid(k_axis<T, NN, W, true, true>, NT, smem, ntiles, c[0]),
-                          NT, smem, st, a, nzt, no, (int)ntiles);
-      return launch_pdl(k_axis<T, NN, W, false, true>, resident_grid(k_axis<T, NN, W, false, true>, NT, smem, ntiles, c[1]),
-                        NT, smem, st, a, nzt, no, (int)ntiles);
+        return launch_pdl(k_axis<T, NN, W, true, 1>, resident_grid(k_axis<T, NN, W, true, 1>, NT, smem, ntiles, c[0]),
+                          NT, smem, st, a, nzt, no, (int)ntiles, mA, mB);
+      return launch_pdl(k_axis<T, NN, W, false, 1>, resident_grid(k_axis<T, NN, W, false, 1>, NT, smem, ntiles, c[1]),
+                        NT, smem, st, a, nzt, no, (int)ntiles, mA, mB);
     } else {
       const size_t smem = axis_smem<T, NN, W, false>();
       if (inv)
-        k_axis<T, NN, W, true, false><<<resident_grid(k_axis<T, NN, W, true, false>, NT, smem, ntiles, c[2]), NT,
-                                        smem, st>>>(a, nzt, no, (int)ntiles);
+        k_axis<T, NN, W, true, 0><<<resident_grid(k_axis<T, NN, W, true, 0>, NT, smem, ntiles, c[2]), NT, smem, st>>>(
+            a, nzt, no, (int)ntiles, mA, mB);
       else
-        k_axis<T, NN, W, false, false><<<resident_grid(k_axis<T, NN, W, false, false>, NT, smem, ntiles, c[3]),
-                                         NT, smem, st>>>(a, nzt, no, (int)ntiles);
+        k_axis<T, NN, W, false, 0><<<resident_grid(k_axis<T, NN, W, false, 0>, NT, smem, ntiles, c[3]), NT, smem,
+                                     st>>>(a, nzt, no, (int)ntiles, mA, mB);
     }
     return cudaGetLastError();
   });
+}
+
+// Read and clear the flag a TMA wait of k_axis sets when it gives up.
+cudaError_t take_axis_timeout(int* flag) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_axis_timeout, sizeof(int));
+  if (e != cudaSuccess) return e;
+  *flag = v;
+  const int zero = 0;
+  return v ? cudaMemcpyToSymbol(g_axis_timeout, &zero, sizeof(int)) : cudaSuccess;
 }
 
 template <typename T> int p3_tile_w(int Nx) {
@@ -748,10 +864,12 @@ template <typename T> cudaError_t prepare_axis_kernels(int Nx) {
     constexpr int NN = decltype(nn)::value;
     cudaError_t e;
     constexpr int W = tile_w<T>(NN);
-    if ((e = max_smem(k_axis<T, NN, W, true, true>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
-    if ((e = max_smem(k_axis<T, NN, W, false, true>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
-    if ((e = max_smem(k_axis<T, NN, W, true, false>, (int)axis_smem<T, NN, W, false>())) != cudaSuccess) return e;
-    return max_smem(k_axis<T, NN, W, false, false>, (int)axis_smem<T, NN, W, false>());
+    if ((e = max_smem(k_axis<T, NN, W, true, 2>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
+    if ((e = max_smem(k_axis<T, NN, W, false, 2>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
+    if ((e = max_smem(k_axis<T, NN, W, true, 1>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
+    if ((e = max_smem(k_axis<T, NN, W, false, 1>, (int)axis_smem<T, NN, W, true>())) != cudaSuccess) return e;
+    if ((e = max_smem(k_axis<T, NN, W, true, 0>, (int)axis_smem<T, NN, W, false>())) != cudaSuccess) return e;
+    return max_smem(k_axis<T, NN, W, false, 0>, (int)axis_smem<T, NN, W, false>());
   });
 }
 

@@ -53,6 +53,7 @@ template <typename T> struct AxisArgs {
   int nz;
   const V2<T>* tw;
   int src_cols;  // entries per source row that may be read (0: nz); staging reads whole W-column tiles
+  int br, ka, kb, pb;  // TMA staging (set by the launcher): box rows, boxes per half, rows of the second half
 };
 
 // P1: x-inverse of the stage input and of curl(u): 3 compact components in,
@@ -141,6 +142,7 @@ template <typename T> cudaError_t prepare_fft_kernels(int Nx, int Ny, int Nz);
 template <typename T> cudaError_t prepare_axis_kernels(int Nx);
 int p3_num_blocks(const Geom& g, int W);
 template <typename T> int p3_tile_w(int Nx);
+cudaError_t take_axis_timeout(int* flag);
 template <typename T> int axis_tile_w(int N);
 
 // ---- reductions / elementwise (k_reduce.cu) ----------------------------------

@@ -1013,6 +1013,13 @@ int hit_rhs(hit_plan* p, const void* u_hat, const hit_params* pr, double t, void
   return DISPATCH(p, rhs_impl)(p, u_hat, pr, du, nullptr, (cudaStream_t)stream);
 }
 
+int hit_device_status(int* status) {
+  if (!status) return fail(HIT_E_INVALID, "NULL argument");
+  cudaError_t e = take_axis_timeout(status);
+  if (e != cudaSuccess) return cuda_fail(e, "device_status");
+  return HIT_OK;
+}
+
 int hit_rhs_forced(hit_plan* p, const void* u_hat, const hit_params* pr, const void* f_ext, double t, void* du,
                    void* stream) {
   (void)t;

@@ -118,6 +118,11 @@ int hit_check_dealiased(hit_plan *plan, const void *u_hat, int *flag_dev,
 int hit_rhs(hit_plan *plan, const void *u_hat, const hit_params *params,
             double t, void *du_hat, void *stream);
 
+/* *status = 1 if a bounded wait of a transform kernel (the TMA tile loads of
+ * the y and x passes) gave up since the last call, else 0; clears it.
+ * Synchronises with the device.  No reference counterpart. */
+int hit_device_status(int *status);
+
 /* rhs and rollout with an external force f_ext (reference layout, device),
  * held constant over the call: rhs = project(dealias(u x w + forcing + f_ext))
  * - nu k^2 u, the RHS of a coarse LES whose subgrid-stress divergence is
