@@ -19,6 +19,7 @@
 
 #include "fft_core.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 namespace hit {
 
@@ -80,6 +81,9 @@ __device__ __forceinline__ void fill_z_twiddles(V2<T>* tws, const V2<T>* __restr
   __syncthreads();
 }
 
+constexpr int Z_WAIT = 1 << 22;  // mbarrier polls before a TMA wait gives up
+__device__ int g_z_timeout = 0;   // set when a TMA wait gave up (hit_device_status)
+
 template <typename T, int H, int RB, int NTZ, int MINB>
 __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -102,34 +106,47 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
   constexpr int NWARP = NTZ / 32;
 
-  // stage the 6 component rows of a group (rows past the end are zero-filled):
-  // a warp per row, a lane per 16-byte chunk
+  // stage the 6 component rows of a group with one bulk TMA copy per row
+  // (Mzp entries, a multiple of 8: whole 16-byte chunks), issued by one thread
+  // and counted on an mbarrier.  Rows past the end are not loaded: their
+  // columns keep stale values, which stay in those columns of the transforms
+  // and are never written out.
+  __shared__ __align__(8) uint64_t zbar;
+  const uint32_t mb = tma::smem_u32(&zbar);
+  if (threadIdx.x == 0) tma::mbar_init(mb, 1);
+  tma::fence_async_smem();
+  __syncthreads();
   auto prefetch = [&](int grp) {
-    const long long r0 = (long long)grp * RB;
-    const int chunks = Mzp / VPC;  // Mzp is a multiple of 8: whole 16-byte chunks
-    for (int col = warp; col < 6 * RB; col += NWARP) {
-      const int q = col / RB, lr = col % RB;
-      V2<T>* dst = raw + col * RS;
-      const bool in = r0 + lr < a.nrows;
-      const V2<T>* src = a.buf + q * a.c_stride + (r0 + lr) * Mzp;
-      for (int ch = lane; ch < chunks; ch += 32) {
-        if (in) cp_async16(dst + ch * VPC, src + ch * VPC);
-        else
-          for (int i = 0; i < VPC; ++i) dst[ch * VPC + i] = czero<T>();
+    if (threadIdx.x == 0) {
+      const long long r0 = (long long)grp * RB;
+      const int nin = (int)(a.nrows - r0 < RB ? a.nrows - r0 : RB);
+      const uint32_t bytes = (uint32_t)(Mzp * sizeof(V2<T>));
+      tma::mbar_expect_tx(mb, 6u * nin * bytes);
+      for (int col = 0; col < 6 * RB; ++col) {
+        const int q = col / RB, lr = col % RB;
+        if (lr < nin) tma::load_bytes(raw + col * RS, a.buf + q * a.c_stride + (r0 + lr) * Mzp, bytes, mb);
       }
     }
-    cp_async_commit();
   };
 
   pdl_wait();
   pdl_trigger();
   int grp = blockIdx.x;
   if (grp < ngroups) prefetch(grp);
+  uint32_t phase = 0;
   for (; grp < ngroups; grp += gridDim.x) {
     const long long row0 = (long long)grp * RB;
     const bool full = row0 + RB <= a.nrows;
-    cp_async_wait_all();
-    __syncthreads();
+    {
+      // the group's rows have landed (a verdict shared by the block)
+      const bool ok = __syncthreads_and(tma::mbar_wait(mb, phase, Z_WAIT)) != 0;
+      phase ^= 1;
+      if (!ok) {
+        if (threadIdx.x == 0) atomicExch(&g_z_timeout, 1);
+        tma::mbar_wait(mb, phase ^ 1, Z_WAIT);  // the copies in flight, once more with a limit
+        return;
+      }
+    }
 
     // c2r of the 6 components of RB rows (column = q*RB + lr) from the staged
     // rows; as soon as every thread holds its first-stage inputs the staging
@@ -295,6 +312,16 @@ __global__ void __launch_bounds__(NTZ) k_zr2c(ZRealArgs<T> a) {
       a.cbuf[c * a.cc_stride + (row0 + lr) * a.Mzp + k] = v;
     }
   }
+}
+
+// Read and clear the flag a TMA wait of k_zcross sets when it gives up.
+cudaError_t take_z_timeout(int* flag) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_z_timeout, sizeof(int));
+  if (e != cudaSuccess) return e;
+  *flag = v;
+  const int zero = 0;
+  return v ? cudaMemcpyToSymbol(g_z_timeout, &zero, sizeof(int)) : cudaSuccess;
 }
 
 template <typename F> cudaError_t dispatch_half(int H, F&& f) {

@@ -143,6 +143,7 @@ template <typename T> cudaError_t prepare_axis_kernels(int Nx);
 int p3_num_blocks(const Geom& g, int W);
 template <typename T> int p3_tile_w(int Nx);
 cudaError_t take_axis_timeout(int* flag);
+cudaError_t take_z_timeout(int* flag);
 template <typename T> int axis_tile_w(int N);
 
 // ---- reductions / elementwise (k_reduce.cu) ----------------------------------

@@ -1015,8 +1015,11 @@ int hit_rhs(hit_plan* p, const void* u_hat, const hit_params* pr, double t, void
 
 int hit_device_status(int* status) {
   if (!status) return fail(HIT_E_INVALID, "NULL argument");
+  int z = 0;
   cudaError_t e = take_axis_timeout(status);
+  if (e == cudaSuccess) e = take_z_timeout(&z);
   if (e != cudaSuccess) return cuda_fail(e, "device_status");
+  *status = *status || z;
   return HIT_OK;
 }
 

@@ -50,6 +50,15 @@ __device__ __forceinline__ void load4(void* dst, const CUtensorMap* map, int x, 
       : "memory");
 }
 
+// Contiguous bytes (16-byte aligned addresses, a multiple of 16 bytes) from
+// global into shared memory, completing on mbar.
+__device__ __forceinline__ void load_bytes(void* dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(mbar)
+      : "memory");
+}
+
 // Generic-proxy shared-memory writes ordered before later async-proxy (TMA)
 // accesses.
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
