@@ -117,12 +117,13 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   tma::fence_async_smem();
   __syncthreads();
   auto prefetch = [&](int grp) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {  // warp 0: lane 0 sets the transaction count, the lanes issue the rows
       const long long r0 = (long long)grp * RB;
       const int nin = (int)(a.nrows - r0 < RB ? a.nrows - r0 : RB);
       const uint32_t bytes = (uint32_t)(Mzp * sizeof(V2<T>));
-      tma::mbar_expect_tx(mb, 6u * nin * bytes);
-      for (int col = 0; col < 6 * RB; ++col) {
+      if (threadIdx.x == 0) tma::mbar_expect_tx(mb, 6u * nin * bytes);
+      __syncwarp();
+      for (int col = threadIdx.x; col < 6 * RB; col += 32) {
         const int q = col / RB, lr = col % RB;
         if (lr < nin) tma::load_bytes(raw + col * RS, a.buf + q * a.c_stride + (r0 + lr) * Mzp, bytes, mb);
       }
