@@ -81,7 +81,7 @@ SIGNATURES = {
     "hit_energy_budget": (_i, [_vp, _vp, _PP, _vp, _vp]),
     "hit_tc_gemm_bf16": (_i, [_vp, _i, _vp, _i, _vp, _i, _i, _i, _i, _vp, _vp]),
     "hit_mlp_forward": (_i, [_vp, _vp, _i64, _vp, _vp, _vp]),
-    "hit_mlp_forward_strided": (_i, [_vp, _vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _vp]),
+    "hit_mlp_forward_strided": (_i, [_vp, _vp, _i64, _i64, _i64, _vp, _i64, _i64, _i, _vp, _vp]),
     "hit_velocity_gradients": (_i, [_vp, _vp, _vp, _vp]),
     "hit_add_sgs_force": (_i, [_vp, _vp, _vp, _vp]),
     "hit_sgs_force": (_i, [_vp, _vp, _vp, _vp]),

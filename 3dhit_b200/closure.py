@@ -127,14 +127,16 @@ class ClosureMLP:
         self._packed = None
         return w
 
-    def forward_fields(self, grads, out):
+    def forward_fields(self, grads, out, ctas_per_sm=0):
         """SGS stress fields out (6, P) from gradient fields grads (9, P)
-        (component-major, physical units, float32 device tensors)."""
+        (component-major, physical units, float32 device tensors);
+        ``ctas_per_sm`` > 0 caps the kernel's CTAs per SM (when it runs beside
+        other work)."""
         if getattr(self, "_physical", None) is None:
             self.pack_physical()
         P = grads.shape[1]
         nat.call("hit_mlp_forward_strided", ctypes_ref(self._physical[0]), nat.ptr(grads), P, 1, P, nat.ptr(out), P, 1,
-                 nat.ptr(self._err), nat.stream_ptr(self.device))
+                 int(ctas_per_sm), nat.ptr(self._err), nat.stream_ptr(self.device))
         return out
 
     def loss_and_grads(self, x, tau):

@@ -273,10 +273,11 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
 size_t mlp_smem_bytes() { return sizeof(MlpSmem<true>); }
 
 // Training pass when a.tau is set, else inference.  grid <= 0: one resident
-// wave of CTAs (at most 8 per SM: 8 x 64 TMEM columns fill the SM's 512).
+// wave of CTAs (at most 8 per SM: 8 x 64 TMEM columns fill the SM's 512), or
+// -k: k CTAs per SM (a lighter footprint next to other work on the GPU).
 cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st) {
   static bool ready[2] = {false, false};
-  static int wave = 0;
+  static int wave = 0, per_sm_wave = 1;
   const bool train = a.tau != nullptr;
   const int smem = train ? (int)sizeof(MlpSmem<true>) : (int)sizeof(MlpSmem<false>);
   if (!ready[train]) {
@@ -304,11 +305,13 @@ cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st) {
       if ((e = cudaFuncGetAttributes(&fa, k_mlp<false>)) != cudaSuccess) return e;
       const int by_smem = smem_sm / (smem + 1024);
       const int by_regs = regs_sm / (128 * ((std::max(fa.numRegs, 1) + 7) / 8 * 8));
-      wave = std::max(1, std::min(std::min(by_smem, by_regs), 8)) * sms;
+      per_sm_wave = std::max(1, std::min(std::min(by_smem, by_regs), 8));
+      wave = per_sm_wave * sms;
     }
     ready[train] = true;
   }
   const long long tiles = (a.P + 127) / 128;
+  if (grid < 0 && !train) grid = (int)std::min<long long>(tiles, std::min(-grid * (wave / per_sm_wave), wave));
   if (grid <= 0) grid = (int)std::min<long long>(tiles, train ? 2 * 148 : wave);
   if (train) k_mlp<true><<<grid, 128, smem, st>>>(a);
   else k_mlp<false><<<grid, 128, smem, st>>>(a);

@@ -57,9 +57,10 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 extern "C" {
 
 int hit_mlp_forward_strided(const hit_mlp_weights* w, const float* x, int64_t x_sf, int64_t x_sp, int64_t P, float* y,
-                            int64_t y_sf, int64_t y_sp, int* err, void* stream) {
+                            int64_t y_sf, int64_t y_sp, int ctas_per_sm, int* err, void* stream) {
   if (!weights_ok(w, false) || !x || !y || !err) return hit::record_error(HIT_E_INVALID, "mlp_forward: NULL argument");
   if (P < 1) return hit::record_error(HIT_E_INVALID, "mlp_forward: P must be >= 1");
+  if (ctas_per_sm < 0) return hit::record_error(HIT_E_INVALID, "mlp_forward: ctas_per_sm must be >= 0");
   MlpArgs a = args_of(w);
   a.x = x;
   a.y = y;
@@ -69,12 +70,13 @@ int hit_mlp_forward_strided(const hit_mlp_weights* w, const float* x, int64_t x_
   a.y_sf = y_sf;
   a.y_sp = y_sp;
   a.err = err;
-  cudaError_t e = hit::launch_mlp(a, 0, (cudaStream_t)stream);  // one resident wave of inference CTAs
+  // one resident wave of inference CTAs, or ctas_per_sm of them per SM
+  cudaError_t e = hit::launch_mlp(a, -ctas_per_sm, (cudaStream_t)stream);
   return e == cudaSuccess ? HIT_OK : cuda_err(e, "mlp_forward");
 }
 
 int hit_mlp_forward(const hit_mlp_weights* w, const float* x, int64_t P, float* y, int* err, void* stream) {
-  return hit_mlp_forward_strided(w, x, 1, 9, P, y, 1, 6, err, stream);
+  return hit_mlp_forward_strided(w, x, 1, 9, P, y, 1, 6, 0, err, stream);
 }
 
 int64_t hit_mlp_workspace_bytes(int64_t P) {

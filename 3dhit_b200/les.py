@@ -133,8 +133,11 @@ class FusedLESStep:
     allocated at construction, so a call can be captured into a CUDA graph
     after one warm-up call."""
 
-    def __init__(self, grid, closure, params, dt, lag=False):
+    def __init__(self, grid, closure, params, dt, lag=False, mlp_ctas_per_sm=2):
         self.grid, self.closure, self.params, self.dt, self.lag = grid, closure, params, float(dt), bool(lag)
+        # with the lag the MLP shares the GPU with the step: a lighter footprint
+        # (fewer CTAs per SM) keeps the step's kernels from waiting for SM space
+        self.mlp_ctas_per_sm = int(mlp_ctas_per_sm) if self.lag else 0
         self.ns = make_ns_rhs(grid)
         P = grid.Nx * grid.Ny * grid.Nz
         dev = grid.device
@@ -163,7 +166,7 @@ class FusedLESStep:
         out = self._f if out is None else out
         st = nat.stream_ptr(g.device)
         nat.call("hit_velocity_gradients", g.plan.handle, nat.ptr(u_hat), nat.ptr(self._grads), st)
-        self.closure.forward_fields(self._grads, self._tau)
+        self.closure.forward_fields(self._grads, self._tau, self.mlp_ctas_per_sm)
         tau_hat = to_spectral(self._tau.reshape(6, g.Nx, g.Ny, g.Nz), g)
         nat.call("hit_sgs_force", g.plan.handle, nat.ptr(tau_hat), nat.ptr(out), st)
         return out

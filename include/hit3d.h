@@ -230,11 +230,13 @@ typedef struct hit_mlp_weights {
 int hit_mlp_forward(const hit_mlp_weights *w, const float *x, int64_t P,
                     float *y, int *err_dev, void *stream);
 /* The same with strided arrays: feature f of point p at x[f*x_sf + p*x_sp],
- * output c at y[c*y_sf + p*y_sp] (component-major fields: x_sf = P, x_sp = 1). */
+ * output c at y[c*y_sf + p*y_sp] (component-major fields: x_sf = P, x_sp = 1).
+ * ctas_per_sm: 0 = as many CTAs as fit (fastest alone); k > 0 = at most k per
+ * SM (a lighter footprint when other kernels run concurrently). */
 int hit_mlp_forward_strided(const hit_mlp_weights *w, const float *x,
                             int64_t x_sf, int64_t x_sp, int64_t P, float *y,
-                            int64_t y_sf, int64_t y_sp, int *err_dev,
-                            void *stream);
+                            int64_t y_sf, int64_t y_sp, int ctas_per_sm,
+                            int *err_dev, void *stream);
 
 /* LES with the closure (no reference counterpart), reference layout:
  * grads_out (DEVICE, 9 x Nx*Ny*Nz, the plan's dtype) receives du_i/dx_j
