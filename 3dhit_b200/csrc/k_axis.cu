@@ -845,17 +845,23 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Ar
                     NTH, smem, st, a, nzt, ntiles);
 }
 
+// Threads per k_p1/k_p3 CTA: 512 (one CTA per SM at 512- and 1024-point
+// columns); 256 for columns of at most 128 points, whose tiles have at most
+// 128 butterflies per stage, so that the CTA leaves half an SM's registers to
+// other work (on small grids, e.g. a closure on a second stream).
+template <int N> constexpr int p_threads() { return N <= 128 ? NTP / 2 : NTP; }
+
 template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st) {
   return dispatch_len(a.g.Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
-    return launch_p1_v<T, NN, tile_wp<T>(NN), NTP>(a, st);
+    return launch_p1_v<T, NN, tile_wp<T>(NN), p_threads<NN>()>(a, st);
   });
 }
 
 template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st) {
   return dispatch_len(a.g.Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
-    return launch_p3_v<T, NN, tile_wp<T>(NN), NTP>(a, st);
+    return launch_p3_v<T, NN, tile_wp<T>(NN), p_threads<NN>()>(a, st);
   });
 }
 

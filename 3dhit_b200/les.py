@@ -133,7 +133,7 @@ class FusedLESStep:
     allocated at construction, so a call can be captured into a CUDA graph
     after one warm-up call."""
 
-    def __init__(self, grid, closure, params, dt, lag=False, mlp_ctas_per_sm=2):
+    def __init__(self, grid, closure, params, dt, lag=False, mlp_ctas_per_sm=1):
         self.grid, self.closure, self.params, self.dt, self.lag = grid, closure, params, float(dt), bool(lag)
         # with the lag the MLP shares the GPU with the step: a lighter footprint
         # (fewer CTAs per SM) keeps the step's kernels from waiting for SM space
