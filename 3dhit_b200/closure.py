@@ -9,7 +9,7 @@ tensor-core kernels behind ``hit_mlp_forward`` / ``hit_mlp_train_grads``
 optimiser on the gradients those kernels return.
 
 The reference has no closure (its LES/closure work is a stated direction of
-the project); this is the north star's learned part.
+the project); this package adds it as the learned part of the solver.
 """
 
 from __future__ import annotations

@@ -16,7 +16,7 @@
 * ``make_dataset`` / ``train`` / ``run_les``: the closure experiment
   (filtered forced DNS -> training -> LES against filtered DNS spectra).
 
-The reference has no LES; this is the north star's learned part built on the
+The reference has no LES; this is the learned part of the package, built on the
 package's own solver and kernels.
 """
 
