@@ -319,19 +319,19 @@ def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20
 
 
 def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5, freeze_every=4,
-            fused=True, lag=False):
+            fused=True, lag=False, forcing=None):
     """Coarse LES from the first filtered snapshot's state with the DNS's
     Lundgren forcing holding the total energy of the filtered DNS field (its
     mean over the snapshots; relaxation time ``tau_relax``), the SGS stress
     evaluated once per RK4 step (``freeze_every`` = 4; `FusedLESStep` when
     ``fused``, else the composed `LESRHS` step; ``lag``: the fused step's
-    lagged closure); returns the time-averaged
+    lagged closure; ``forcing`` replaces the hold-energy forcing); returns the time-averaged
     spectrum over the samples after ``discard`` steps, the step time and the
     energy history."""
     coarse = data["coarse"]
     kc = coarse.Nx // 3
     E_res = sum(data["E_filtered"]) / len(data["E_filtered"])
-    p = NSParams(nu=data["nu"], forcing=HoldEnergyForcing(E_res, data["nu"], tau=tau_relax))
+    p = NSParams(nu=data["nu"], forcing=forcing or HoldEnergyForcing(E_res, data["nu"], tau=tau_relax))
     u = data["u0_coarse"].clone()
     dt = data.get("dt_les") or cfl_dt(u, coarse, 0.5)
     if fused and freeze_every == 4:

@@ -412,6 +412,47 @@ def run_config2(args):
     return 0
 
 
+def closure_diagnosis(les, data, model, args):
+    """Where the LES spectrum error comes from: the drift of the filtered DNS
+    spectrum over its snapshots; the LES over exactly the DNS's sampling window
+    (LES samples at the snapshot times, dt = 1/12 of the snapshot interval);
+    the LES under other forcings (hold-energy with relaxation time 0.05, and a
+    constant Lundgren coefficient equal to the DNS's mean); the closure scaled
+    by 0.7 and 1.4."""
+    fmod = importlib.import_module("3dhit_b200.forcing")
+    S = data["spectra"]
+    q = max(1, S.shape[0] // 5)
+
+    def r4(t):
+        return [round(float(x), 4) for x in t]
+
+    def errs(ratio):
+        return {"max": round(float((ratio - 1).abs().max()), 4), "mean": round(float((ratio - 1).abs().mean()), 4),
+                "ratio_Ek": r4(ratio)}
+
+    out = {"dns_first_fifth": r4(S[:q].mean(0)), "dns_last_fifth": r4(S[-q:].mean(0)),
+           "dns_A_first_last": [data["A"][0], data["A"][-1]]}
+    ref = S.mean(0)
+    m = 12
+    win = dict(data, dt_les=args.cl_every * data["dt"] / m)
+    for name, cl in (("no_closure", None), ("closure", model)):
+        r = les.run_les(win, cl, steps=m * (S.shape[0] - 1), sample_every=m, discard=0)
+        out["same_window_" + name] = errs(r["spectrum"] / S[1:].mean(0))
+    nu, E_res = data["nu"], sum(data["E_filtered"]) / len(data["E_filtered"])
+    A_mean = sum(data["A"]) / len(data["A"])
+    base = model.sgs_scale
+    for name, forcing, sc in (("holdE_tau0.05", fmod.HoldEnergyForcing(E_res, nu, tau=0.05), 1.0),
+                              ("linear_meanA", fmod.LinearForcing(A=A_mean), 1.0),
+                              ("linear_meanA_scale0.7", fmod.LinearForcing(A=A_mean), 0.7),
+                              ("linear_meanA_scale1.4", fmod.LinearForcing(A=A_mean), 1.4)):
+        model.sgs_scale, model._physical = base * sc, None
+        r = les.run_les(data, model, steps=args.cl_les_steps, discard=args.cl_les_steps // 5, forcing=forcing)
+        out["closure_" + name] = dict(errs(r["spectrum"] / ref), energy_first_last=[r["energies"][0],
+                                                                                     r["energies"][-1]])
+    model.sgs_scale, model._physical = base, None
+    return out
+
+
 def run_closure(args):
     """Learned SGS closure (Lundgren hold-energy forced DNS on F^3, sharp
     spectral filter to C^3 at k_c = C/3, MLP 9 -> 64x3 -> 6 on the tensor
@@ -456,6 +497,8 @@ def run_closure(args):
             "dns_ms_per_step": data["dns_ms_per_step"], "dns_dt": data["dt"], "mean_A": sum(data["A"]) / len(data["A"]),
             "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train},
             "no_closure": out["no_closure"], "closure": out["closure"], "closure_lagged": out["closure_lagged"]}
+    if args.cl_diagnose:
+        line["diagnosis"] = closure_diagnosis(les, data, model, args)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -492,6 +535,8 @@ def main():
     ap.add_argument("--cl-every", type=int, default=50)
     ap.add_argument("--cl-train-steps", type=int, default=400)
     ap.add_argument("--cl-les-steps", type=int, default=5000)
+    ap.add_argument("--cl-diagnose", action="store_true",
+                    help="closure run: add the spectrum-error diagnosis (DNS drift, same-window LES, other forcings)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
