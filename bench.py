@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import importlib
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -412,13 +413,42 @@ def run_config2(args):
     return 0
 
 
+def spectral_eddy_viscosity_les(data, steps, discard, coef=1.0, sample_every=50):
+    """The coarse LES with a classical spectral closure instead of the MLP:
+    the Chollet-Lesieur eddy viscosity nu_t(k) = coef C_K^(-3/2) (0.441 + 15.2
+    exp(-3.03 k_c / k)) sqrt(E(k_c) / k_c) (C_K = 1.4, E(k_c) the LES's own
+    shell-k_c energy each step), applied as the force -nu_t(k) k^2 u_hat held
+    over each RK4 step, under the same hold-energy forcing as `les.run_les`.
+    Returns the time-averaged spectrum of shells 1..k_c."""
+    h3 = importlib.import_module("3dhit_b200")
+    fmod = importlib.import_module("3dhit_b200.forcing")
+    g, nu = data["coarse"], data["nu"]
+    kc = g.Nx // 3
+    E_res = sum(data["E_filtered"]) / len(data["E_filtered"])
+    p = h3.NSParams(nu=nu, forcing=fmod.HoldEnergyForcing(E_res, nu, tau=0.5))
+    shape = coef * 1.4 ** -1.5 * (0.441 + 15.2 * torch.exp(-3.03 * kc / g.k2.sqrt().clamp_min(1e-6)))
+    rhs = h3.make_ns_rhs(g)
+    u = data["u0_coarse"].clone()
+    dt = h3.cfl_dt(u, g, 0.5)
+    spec, n = torch.zeros(kc, dtype=torch.float64), 0
+    for i in range(1, steps + 1):
+        Ekc = max(float(h3.energy_spectrum(u, g)[1][kc - 1]), 0.0)
+        f = (-(shape * g.k2) * math.sqrt(Ekc / kc)).to(u.dtype) * u
+        u = h3.rk4_step(rhs, u, p, dt, 0.0, f_ext=f)
+        if i % sample_every == 0 and i > discard:
+            spec += torch.as_tensor(h3.energy_spectrum(u, g)[1][:kc], dtype=torch.float64)
+            n += 1
+    return spec / max(n, 1)
+
+
 def closure_diagnosis(les, data, model, args):
     """Where the LES spectrum error comes from: the drift of the filtered DNS
     spectrum over its snapshots; the LES over exactly the DNS's sampling window
     (LES samples at the snapshot times, dt = 1/12 of the snapshot interval);
     the LES under other forcings (hold-energy with relaxation time 0.05, and a
     constant Lundgren coefficient equal to the DNS's mean); the closure scaled
-    by 0.7 and 1.4."""
+    by 0.7 and 1.4; the classical Chollet-Lesieur spectral eddy viscosity in
+    place of the MLP (coefficient 1 and 0.5)."""
     fmod = importlib.import_module("3dhit_b200.forcing")
     S = data["spectra"]
     q = max(1, S.shape[0] // 5)
@@ -450,6 +480,9 @@ def closure_diagnosis(les, data, model, args):
         out["closure_" + name] = dict(errs(r["spectrum"] / ref), energy_first_last=[r["energies"][0],
                                                                                      r["energies"][-1]])
     model.sgs_scale, model._physical = base, None
+    for coef in (1.0, 0.5):
+        spec = spectral_eddy_viscosity_les(data, args.cl_les_steps, args.cl_les_steps // 5, coef=coef)
+        out[f"chollet_lesieur_{coef}"] = errs(spec / ref)
     return out
 
 
