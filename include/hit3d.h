@@ -211,7 +211,7 @@ int hit_energy_budget(hit_plan *plan, const void *u_hat,
 int hit_tc_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C,
                      int ldc, int M, int N, int K, int *err_dev, void *stream);
 
-/* Learned subgrid-stress closure (north-star closure; no reference
+/* Learned subgrid-stress closure for the coarse LES (no reference
  * counterpart): pointwise MLP 9 -> 64 -> 64 -> 64 -> 6 with GELU, bf16 weights
  * and activations, float32 accumulation, on the tcgen05 tensor cores.  Input
  * per point: the 9 filtered velocity-gradient components du_i/dx_j (i-major);
