@@ -8,6 +8,7 @@ arrays.  The package directory name starts with a digit, so import it with
 ``importlib.import_module("3dhit_b200")``.
 """
 
+from ._native import DeviceWaitError, check_device
 from .callbacks import Callback, Diagnostic, FieldWriter, State, save_series
 from .diagnostics import (
     compensated_spectrum,
@@ -69,5 +70,5 @@ __all__ = [
     "compensated_spectrum", "dissipation_constant", "kolmogorov_scale",
     "taylor_microscale", "taylor_reynolds", "taylor_reynolds_field", "energy_budget",
     "energy_budget_cb", "velocity_samples", "velocity_moments",
-    "longitudinal_autocorrelation", "integral_lengthscale",
+    "longitudinal_autocorrelation", "integral_lengthscale", "check_device", "DeviceWaitError",
 ]

@@ -72,6 +72,7 @@ SIGNATURES = {
     "hit_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _d, _vp, _vp]),
     "hit_rhs_forced": (_i, [_vp, _vp, _PP, _vp, _d, _vp, _vp]),
     "hit_device_status": (_i, [ctypes.POINTER(ctypes.c_int)]),
+    "hit_set_wait_limit": (_i, [_i]),
     "hit_rollout_forced": (_i, [_vp, _vp, _PP, _vp, _d, _i64, _d, _vp, _vp]),
     "hit_profile_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _vp, _vp, _vp, _vp]),
     "hit_rhs_vjp": (_i, [_vp, _vp, _PP, _d, _vp, _vp, _vp, _vp]),
@@ -138,6 +139,22 @@ def call(name, *args):
             raise ValueError(f"{name}: {msg}")
         raise HitError(name, rc, msg)
     return rc
+
+
+class DeviceWaitError(RuntimeError):
+    """A bounded wait inside a transform kernel gave up: the results of the
+    calls since the last check are not valid."""
+
+
+def check_device(where=""):
+    """Raise `DeviceWaitError` if a bounded TMA wait of a transform pass gave
+    up since the last check (``hit_device_status``, which reads and clears
+    the flag; it synchronises with the current device)."""
+    st = ctypes.c_int(0)
+    call("hit_device_status", ctypes.byref(st))
+    if st.value:
+        raise DeviceWaitError(f"a TMA tile wait of a transform kernel gave up{' in ' + where if where else ''}; "
+                              "the results since the last check are not valid")
 
 
 def stream_ptr(device):

@@ -64,6 +64,10 @@ struct TileWalk {
 // forward one always reads all N rows (the launcher checks this).
 constexpr int AXIS_WAIT = 1 << 22;  // mbarrier polls before a TMA wait gives up
 __device__ int g_axis_timeout = 0;  // set when a TMA wait gave up (hit_device_status)
+// Polls of the wait for a tile's boxes (hit_set_wait_limit lowers it so that
+// a test can make the wait give up); the wait for the copies still in flight
+// after a give-up always polls AXIS_WAIT times.
+__device__ int g_axis_wait_limit = AXIS_WAIT;
 
 template <typename T, int N, int W, bool INV, int PF>
 __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int ntiles,
@@ -108,6 +112,7 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
     tma::fence_async_smem();
   }
   TileWalk walk(blockIdx.x, gridDim.x, nzt, no);
+  const int wait_limit = PF == 2 ? g_axis_wait_limit : 0;
   pdl_wait();
   pdl_trigger();
   __syncthreads();
@@ -125,7 +130,7 @@ __global__ void __launch_bounds__(NT) k_axis(AxisArgs<T> a, int nzt, int no, int
       __syncthreads();
     } else if constexpr (PF == 2) {
       // the tile's boxes have landed (a verdict shared by the block)
-      const bool ok = __syncthreads_and(tma::mbar_wait(mb, phase, AXIS_WAIT)) != 0;
+      const bool ok = __syncthreads_and(tma::mbar_wait(mb, phase, wait_limit)) != 0;
       phase ^= 1;
       if (!ok) {
         if (threadIdx.x == 0) atomicExch(&g_axis_timeout, 1);
@@ -744,7 +749,7 @@ cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, 
     const bool pf = (sizeof(V2<T>) == 16 || ((a.s_a | a.s_o | a.s_c) % 2 == 0 &&
                                               ((uintptr_t)a.src % 16) == 0)) &&
                     (long long)nzt * W <= (a.src_cols > 0 ? a.src_cols : a.nz);
-    static int c[6] = {0, 0, 0, 0, 0, 0};
+    static PerDevice c[6];
     CUtensorMap mA{}, mB{};
     if (pf) {
       // TMA staging when the layout has a tensor map: box rows br (a power of
@@ -787,6 +792,13 @@ cudaError_t launch_axis(int N, bool inv, const AxisArgs<T>& a, int nzt, int no, 
   });
 }
 
+// Polls of the tile-box wait of k_axis on the current device (polls < 0: the
+// default).
+cudaError_t set_axis_wait_limit(int polls) {
+  const int v = polls < 0 ? AXIS_WAIT : polls;
+  return cudaMemcpyToSymbol(g_axis_wait_limit, &v, sizeof(int));
+}
+
 // Read and clear the flag a TMA wait of k_axis sets when it gives up.
 cudaError_t take_axis_timeout(int* flag) {
   int v = 0;
@@ -818,13 +830,9 @@ template <typename K> cudaError_t max_smem(K kernel, int bytes) {
 }
 
 template <typename T, int NN, int W, int NTH> cudaError_t launch_p1_v(const P1Args<T>& a, cudaStream_t st) {
-  static int cache = 0;
-  static bool ready = false;
-  if (!ready) {
-    cudaError_t e = max_smem(k_p1<T, NN, W, NTH>, (int)p1_smem<T, NN>(W));
-    if (e != cudaSuccess) return e;
-    ready = true;
-  }
+  static PerDevice cache, ready;
+  cudaError_t e = once_per_device(ready, [] { return max_smem(k_p1<T, NN, W, NTH>, (int)p1_smem<T, NN>(W)); });
+  if (e != cudaSuccess) return e;
   const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
   const size_t smem = p1_smem<T, NN>(W);
   return launch_pdl(k_p1<T, NN, W, NTH>, resident_grid(k_p1<T, NN, W, NTH>, NTH, smem, ntiles, cache), NTH, smem, st, a,
@@ -832,13 +840,10 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p1_v(const P1Ar
 }
 
 template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Args<T>& a, cudaStream_t st) {
-  static int cache = 0;
-  static bool ready = false;
-  if (!ready) {
-    cudaError_t e = max_smem(k_p3<T, NN, W, NTH>, (int)p3_smem<T, NN, W, NTH>(NN));
-    if (e != cudaSuccess) return e;
-    ready = true;
-  }
+  static PerDevice cache, ready;
+  cudaError_t e =
+      once_per_device(ready, [] { return max_smem(k_p3<T, NN, W, NTH>, (int)p3_smem<T, NN, W, NTH>(NN)); });
+  if (e != cudaSuccess) return e;
   const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
   const size_t smem = p3_smem<T, NN, W, NTH>(a.g.Mx);
   return launch_pdl(k_p3<T, NN, W, NTH>, resident_grid(k_p3<T, NN, W, NTH>, NTH, p3_smem<T, NN, W, NTH>(NN), ntiles, cache),

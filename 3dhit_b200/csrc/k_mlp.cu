@@ -276,22 +276,30 @@ size_t mlp_smem_bytes() { return sizeof(MlpSmem<true>); }
 // wave of CTAs (at most 8 per SM: 8 x 64 TMEM columns fill the SM's 512), or
 // -k: k CTAs per SM (a lighter footprint next to other work on the GPU).
 cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st) {
-  static bool ready[2] = {false, false};
-  static int wave = 0, per_sm_wave = 1;
+  // per device: the attribute set-up of each instantiation, and the
+  // inference wave (CTAs per SM, and that times the SM count)
+  static PerDevice ready[2], wave_of, per_sm_of;
   const bool train = a.tau != nullptr;
   const int smem = train ? (int)sizeof(MlpSmem<true>) : (int)sizeof(MlpSmem<false>);
-  if (!ready[train]) {
+  cudaError_t e = once_per_device(ready[train], [&] {
     // the largest shared-memory carveout, so that the occupancy below (and the
     // launch) can place several CTAs per SM
     auto setup = [&](auto kernel) {
-      cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      if (e != cudaSuccess) return e;
+      cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (r != cudaSuccess) return r;
       return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared);
     };
-    cudaError_t e = train ? setup(k_mlp<true>) : setup(k_mlp<false>);
-    if (e != cudaSuccess) return e;
-    if (!train) {
+    return train ? setup(k_mlp<true>) : setup(k_mlp<false>);
+  });
+  if (e != cudaSuccess) return e;
+  int wave = 0, per_sm_wave = 1;
+  if (!train) {
+    std::atomic<int>* ws = wave_of.here();
+    std::atomic<int>* ps = per_sm_of.here();
+    wave = ws ? ws->load(std::memory_order_relaxed) : 0;
+    per_sm_wave = ps ? ps->load(std::memory_order_relaxed) : 0;
+    if (wave == 0 || per_sm_wave == 0) {
       // CTAs per SM from the SM's shared memory and registers (1 KB of
       // shared memory per CTA is the driver's)
       int dev = 0, sms = 0, smem_sm = 0, regs_sm = 0;
@@ -307,8 +315,9 @@ cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st) {
       const int by_regs = regs_sm / (128 * ((std::max(fa.numRegs, 1) + 7) / 8 * 8));
       per_sm_wave = std::max(1, std::min(std::min(by_smem, by_regs), 8));
       wave = per_sm_wave * sms;
+      if (ps) ps->store(per_sm_wave, std::memory_order_relaxed);
+      if (ws) ws->store(wave, std::memory_order_relaxed);
     }
-    ready[train] = true;
   }
   const long long tiles = (a.P + 127) / 128;
   if (grid < 0 && !train) grid = (int)std::min<long long>(tiles, std::min(-grid * (wave / per_sm_wave), wave));

@@ -83,6 +83,10 @@ __device__ __forceinline__ void fill_z_twiddles(V2<T>* tws, const V2<T>* __restr
 
 constexpr int Z_WAIT = 1 << 22;  // mbarrier polls before a TMA wait gives up
 __device__ int g_z_timeout = 0;   // set when a TMA wait gave up (hit_device_status)
+// Polls of the wait for a row group (hit_set_wait_limit lowers it so that a
+// test can make the wait give up); the wait for the copies still in flight
+// after a give-up always polls Z_WAIT times.
+__device__ int g_z_wait_limit = Z_WAIT;
 
 template <typename T, int H, int RB, int NTZ, int MINB>
 __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
@@ -130,6 +134,7 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
     }
   };
 
+  const int wait_limit = g_z_wait_limit;
   pdl_wait();
   pdl_trigger();
   int grp = blockIdx.x;
@@ -140,7 +145,7 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
     const bool full = row0 + RB <= a.nrows;
     {
       // the group's rows have landed (a verdict shared by the block)
-      const bool ok = __syncthreads_and(tma::mbar_wait(mb, phase, Z_WAIT)) != 0;
+      const bool ok = __syncthreads_and(tma::mbar_wait(mb, phase, wait_limit)) != 0;
       phase ^= 1;
       if (!ok) {
         if (threadIdx.x == 0) atomicExch(&g_z_timeout, 1);
@@ -315,6 +320,13 @@ __global__ void __launch_bounds__(NTZ) k_zr2c(ZRealArgs<T> a) {
   }
 }
 
+// Polls of the row-group wait of k_zcross on the current device (polls < 0:
+// the default).
+cudaError_t set_z_wait_limit(int polls) {
+  const int v = polls < 0 ? Z_WAIT : polls;
+  return cudaMemcpyToSymbol(g_z_wait_limit, &v, sizeof(int));
+}
+
 // Read and clear the flag a TMA wait of k_zcross sets when it gives up.
 cudaError_t take_z_timeout(int* flag) {
   int v = 0;
@@ -348,17 +360,16 @@ template <typename T, int H> constexpr size_t zreal_smem() {
 }
 
 template <typename T, int HH, int RB, int NTZ, int MINB> cudaError_t launch_zcross_v(const ZCrossArgs<T>& a, cudaStream_t st) {
-  static bool ready = false;
+  static PerDevice ready, cache;
   const size_t smem = sizeof(V2<T>) * (6 * RB * skew_ld(HH) + z_tw_slots<HH>() + 6 * RB * z_row_cap<HH>());
-  static int cache = 0;
-  if (!ready) {
-    cudaError_t e = cudaFuncSetAttribute(k_zcross<T, HH, RB, NTZ, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_zcross<T, HH, RB, NTZ, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
-    ready = true;
-  }
+  cudaError_t e = once_per_device(ready, [&] {
+    cudaError_t r = cudaFuncSetAttribute(k_zcross<T, HH, RB, NTZ, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (r != cudaSuccess) return r;
+    return cudaFuncSetAttribute(k_zcross<T, HH, RB, NTZ, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
+  });
+  if (e != cudaSuccess) return e;
   const int nb = resident_grid(k_zcross<T, HH, RB, NTZ, MINB>, NTZ, smem, (a.nrows + RB - 1) / RB, cache);
   return launch_pdl(k_zcross<T, HH, RB, NTZ, MINB>, nb, NTZ, smem, st, a);
 }
@@ -376,7 +387,7 @@ template <typename T, bool C2R> cudaError_t launch_zreal(int H, const ZRealArgs<
     constexpr int HH = decltype(hh)::value;
     constexpr int RB = z_rows_per_block<HH>(), NTZ = z_threads<HH>();
     if (a.Mzp > z_row_cap<HH>()) return cudaErrorInvalidValue;
-    static int cache = 0;
+    static PerDevice cache;
     const long long work = (a.nrows + RB - 1) / RB * ncomp;
     const int grid = resident_grid(k_zreal<T, HH, RB, NTZ, C2R>, NTZ, zreal_smem<T, HH>(), work, cache);
     k_zreal<T, HH, RB, NTZ, C2R><<<grid, NTZ, zreal_smem<T, HH>(), st>>>(a, ncomp);

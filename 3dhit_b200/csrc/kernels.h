@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <utility>
 
 #include <cuda_bf16.h>
@@ -118,17 +119,50 @@ template <typename T> struct ZRealArgs {
   const V2<T>* tw;
 };
 
+// One int per device ordinal, 0 until set.  Kernel attributes (the dynamic
+// shared-memory opt-in, the carveout), occupancy and SM counts belong to one
+// device's context, so launchers keep their one-time set-up and cached launch
+// sizes per device.  The slots are atomic: host threads launching on the same
+// device may both run the first set-up, which is idempotent.  Devices past
+// kMaxDevices get no slot and redo the set-up on every launch.
+constexpr int kMaxDevices = 64;
+struct PerDevice {
+  std::atomic<int> v[kMaxDevices];
+  PerDevice() {
+    for (auto& x : v) x.store(0, std::memory_order_relaxed);
+  }
+  std::atomic<int>* here() {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) return nullptr;
+    return &v[d];
+  }
+};
+
+// Runs f() (returning cudaError_t) once per device; a failed f is retried on
+// the next call.
+template <typename F> cudaError_t once_per_device(PerDevice& done, F&& f) {
+  std::atomic<int>* s = done.here();
+  if (s && s->load(std::memory_order_acquire)) return cudaSuccess;
+  const cudaError_t e = f();
+  if (e == cudaSuccess && s) s->store(1, std::memory_order_release);
+  return e;
+}
+
 // Persistent launch size: the number of blocks that stay resident (the FFT
-// kernels loop over their tiles, filling their shared twiddle tables once).
-template <typename K> int resident_grid(K kernel, int threads, size_t smem, long long ntiles, int& cache) {
-  if (cache == 0) {
+// kernels loop over their tiles, filling their shared twiddle tables once),
+// cached per device.
+template <typename K> int resident_grid(K kernel, int threads, size_t smem, long long ntiles, PerDevice& cache) {
+  std::atomic<int>* slot = cache.here();
+  int n = slot ? slot->load(std::memory_order_relaxed) : 0;
+  if (n == 0) {
     int dev = 0, sms = 0, occ = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem);
-    cache = (occ > 0 ? occ : 1) * (sms > 0 ? sms : 1);
+    n = (occ > 0 ? occ : 1) * (sms > 0 ? sms : 1);
+    if (slot) slot->store(n, std::memory_order_relaxed);
   }
-  return (int)(ntiles < cache ? (ntiles > 0 ? ntiles : 1) : cache);
+  return (int)(ntiles < n ? (ntiles > 0 ? ntiles : 1) : n);
 }
 
 // Launchers (return cudaError_t of the launch).
@@ -144,6 +178,8 @@ int p3_num_blocks(const Geom& g, int W);
 template <typename T> int p3_tile_w(int Nx);
 cudaError_t take_axis_timeout(int* flag);
 cudaError_t take_z_timeout(int* flag);
+cudaError_t set_axis_wait_limit(int polls);
+cudaError_t set_z_wait_limit(int polls);
 template <typename T> int axis_tile_w(int N);
 
 // ---- reductions / elementwise (k_reduce.cu) ----------------------------------

@@ -1023,6 +1023,12 @@ int hit_device_status(int* status) {
   return HIT_OK;
 }
 
+int hit_set_wait_limit(int polls) {
+  cudaError_t e = set_axis_wait_limit(polls);
+  if (e == cudaSuccess) e = set_z_wait_limit(polls);
+  return e == cudaSuccess ? HIT_OK : cuda_fail(e, "set_wait_limit");
+}
+
 int hit_rhs_forced(hit_plan* p, const void* u_hat, const hit_params* pr, const void* f_ext, double t, void* du,
                    void* stream) {
   (void)t;

@@ -13,12 +13,16 @@
 // library until the process exits.
 //
 // Set-up: the first call on a device (with that device current) looks up the
-// device address of the array with cudaGetSymbolAddress and caches it; make
-// that first call before any stream capture.  Every later call reuses the
+// device address of the array with cudaGetSymbolAddress and caches it with the
+// context it was looked up in; make that first call before any stream capture.
+// A call that finds another context current on the device (the old one was
+// torn down, e.g. by cudaDeviceReset) looks the address up again, so a stale
+// address of a module that no longer exists is never used.  Every later call reuses the
 // same array, so calls whose kernels overlap on the GPU (different streams, or
 // different host threads) race on it and must be ordered by the caller.
 // Nothing in the array has to start at zero: every block overwrites all of its
 // partial slots before the finishing kernel reads them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -38,12 +42,30 @@ namespace {
 
 constexpr int kScratchDoubles = 1 << 19;  // 4 MiB of float64 partial sums
 constexpr int kBlocks = 148;              // one block per SM
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_spectrum_scratch[kScratchDoubles];
 
 std::mutex g_mu;
 void* g_scratch_addr[kMaxDevices] = {};
+CUcontext g_scratch_ctx[kMaxDevices] = {};
+
+// The calling thread's current driver context, through the runtime's driver
+// entry point (no link to the driver library); nullptr if unavailable.
+CUcontext current_context() {
+  typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      return reinterpret_cast<CtxGetCurrentFn>(p);
+    cudaGetLastError();
+    return (CtxGetCurrentFn) nullptr;
+  }();
+  CUcontext c = nullptr;
+  if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+  return c;
+}
 
 __device__ __forceinline__ int freq_i(int i, int n) { return i < n / 2 ? i : i - n; }
 
@@ -134,12 +156,15 @@ extern "C" int hit_energy_spectrum_noalloc(int nx, int ny, int nz, double lx, do
   void* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
+    const CUcontext ctx = current_context();
+    if (!g_scratch_addr[dev] || ctx != g_scratch_ctx[dev]) {
+      g_scratch_addr[dev] = nullptr;
       e = cudaGetSymbolAddress(&g_scratch_addr[dev], g_spectrum_scratch);
       if (e != cudaSuccess) {
         g_scratch_addr[dev] = nullptr;
         return record_error(HIT_E_CUDA, std::string("cudaGetSymbolAddress(g_spectrum_scratch): ") + cudaGetErrorString(e));
       }
+      g_scratch_ctx[dev] = current_context();  // the runtime has made the device's primary context current
     }
     scratch = g_scratch_addr[dev];
   }

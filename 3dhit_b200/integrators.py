@@ -6,7 +6,7 @@ of one RK4 step ``nsteps`` times on the current stream with no host
 synchronisation (the replacement for the jitted ``lax.scan``).  Any other
 ``rhs`` callable is integrated by composing its calls with the reference's
 stage algebra.  ``evolve`` is the host loop over rollout segments with
-callbacks (integrators.py:56-109).
+callbacks (reference interface: integrators.py:56-109).
 """
 
 from __future__ import annotations
@@ -154,61 +154,87 @@ def rollout(rhs, u_hat, params, dt, nsteps, t0=0.0, *, assume_dealiased=None, sc
     return u_hat
 
 
+def _progress_interval(progress, nsteps):
+    """Steps between progress lines: 0 = silent; True = about 20 lines."""
+    if progress is True:
+        return max(nsteps // 20, 1)
+    if progress is False or progress is None:
+        return 0
+    return max(int(progress), 1)
+
+
+class _ProgressLine:
+    """One line per report: step, percentage, simulation time, wall time, an
+    estimate of the time left and the step rate."""
+
+    def __init__(self, nsteps):
+        self.nsteps = nsteps
+        self.start = time.perf_counter()
+
+    @staticmethod
+    def _clock(sec):
+        m, s = divmod(sec, 60.0)
+        return f"{s:.1f}s" if m == 0 else f"{int(m)}m{int(round(s)):02d}s"
+
+    def report(self, n, t):
+        wall = time.perf_counter() - self.start
+        left = wall * (self.nsteps - n) / n
+        pct = int(round(100.0 * n / self.nsteps))
+        print(f"step {n}/{self.nsteps} ({pct:3d}%)  t = {t:.6g}  wall {self._clock(wall)}  "
+              f"eta {self._clock(left)}  [{n / max(wall, 1e-9):.1f} steps/s]", flush=True)
+
+
+def _firing_plan(callbacks, nsteps, t0, dt):
+    """{step: callbacks due at that step}, asking each callback once per step
+    (the step's time is t0 + n dt, as the rollout segments see it)."""
+    plan = {}
+    for n in range(nsteps + 1):
+        t = t0 + n * dt
+        due = [cb for cb in callbacks if cb.is_due(n, t, dt)]
+        if due:
+            plan[n] = due
+    return plan
+
+
 def evolve(rhs, u_hat, params, grid, dt, nsteps, *, t0=0.0, callbacks=(), progress=False, scheme="rk4"):
-    """Observation driver (integrators.py:56-109): rollout segments between
-    callback firings, callbacks fired on the segment boundaries; ``scheme``
-    as in `rollout`."""
-    if isinstance(progress, bool):
-        print_every = max(1, nsteps // 20) if progress else 0
-    else:
-        print_every = max(int(progress), 1)
+    """Advance `nsteps` steps while firing callbacks (reference interface:
+    src/hit3d/integrators.py:56-109; ``scheme`` as in `rollout`).
 
-    def due_any(n):
-        t = t0 + n * dt
-        return any(cb.is_due(n, t, dt) for cb in callbacks)
+    The firing plan is made up front (each callback asked once per step);
+    the run is then a chain of `rollout` segments, each ending on a step
+    where a callback fires or a progress line is due, and callbacks see a
+    `State` of that step.  No host synchronisation is added between segments:
+    `Diagnostic` defers its device reads and `FieldWriter` stages snapshots
+    through pinned memory, so the GPU runs the segments back to back.  At the
+    end every callback is finalised and the transform kernels' wait flag is
+    checked (raises `DeviceWaitError` if a bounded wait gave up)."""
+    nsteps = int(nsteps)
+    every = _progress_interval(progress, nsteps)
+    plan = _firing_plan(callbacks, nsteps, t0, dt)
+    stops = set(plan) | ({nsteps} if nsteps > 0 else set())
+    if every:
+        stops |= set(range(every, nsteps + 1, every))
+    stops.discard(0)
+    line = _ProgressLine(nsteps) if every else None
 
-    stops = sorted(
-        {n for n in range(1, nsteps + 1) if due_any(n)}
-        | ({n for n in range(print_every, nsteps + 1, print_every)} if print_every else set())
-        | {nsteps}
-    ) if nsteps > 0 else []
+    def fire(n, u):
+        for cb in plan.get(n, ()):
+            cb.fire(State(u_hat=u, t=t0 + n * dt, step=n, params=params, grid=grid))
 
-    def fire(n):
-        if not callbacks:
-            return
-        t = t0 + n * dt
-        state = State(u_hat=u_hat, t=t, step=n, params=params, grid=grid)
-        for cb in callbacks:
-            if cb.is_due(n, t, dt):
-                cb.fire(state)
-
-    wall0 = time.time()
-    fire(0)
-    prev = 0
-    dealiased = None
-    for n in stops:
-        if _fused(rhs, params) and dealiased is None:
+    fire(0, u_hat)
+    done = 0
+    dealiased = None  # decided once (one device check) for the fused path
+    for n in sorted(stops):
+        if dealiased is None and _fused(rhs, params):
             dealiased = bool(resolve_flags(_check_state(u_hat, grid), grid, None))
-        u_hat = rollout(rhs, u_hat, params, dt, n - prev, t0 + prev * dt, assume_dealiased=dealiased,
-                        scheme=scheme)
-        fire(n)
-        if print_every and (n % print_every == 0 or n == nsteps):
-            _print_progress(n, nsteps, t0 + n * dt, wall0)
-        prev = n
+        u_hat = rollout(rhs, u_hat, params, dt, n - done, t0 + done * dt, assume_dealiased=dealiased, scheme=scheme)
+        fire(n, u_hat)
+        if line is not None and (n % every == 0 or n == nsteps):
+            line.report(n, t0 + n * dt)
+        done = n
     for cb in callbacks:
         cb.finalize()
+    if isinstance(u_hat, torch.Tensor) and u_hat.is_cuda:
+        with torch.cuda.device(u_hat.device):
+            nat.check_device("evolve")
     return u_hat
-
-
-def _print_progress(n, nsteps, t, wall0):
-    elapsed = time.time() - wall0
-    eta = elapsed / n * (nsteps - n)
-    width = len(str(nsteps))
-    print(f"step {n:{width}d}/{nsteps} ({round(100 * n / nsteps):3d}%)  "
-          f"t = {t:<9.4g}  elapsed {_fmt_secs(elapsed)}  eta {_fmt_secs(eta)}", flush=True)
-
-
-def _fmt_secs(s):
-    if s < 60:
-        return f"{s:.1f}s"
-    return f"{int(s // 60)}m{round(s % 60):02d}s"

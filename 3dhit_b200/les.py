@@ -390,5 +390,8 @@ def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True
         u = run(u)
     e1.record()
     torch.cuda.synchronize()
+    nat.check_device("run_les")
+    if closure is not None and hasattr(closure, "check_errors"):
+        closure.check_errors()
     return dict(spectrum=spec / max(n, 1), ms_per_step=e0.elapsed_time(e1) / 200, dt=dt, energies=energies,
                 finite=bool(torch.isfinite(u).all()))

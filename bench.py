@@ -413,6 +413,61 @@ def run_config2(args):
     return 0
 
 
+def run_fp64_compare(args):
+    """Config 3's precision statement: the band-forced N^3 run (BandForcing
+    eps=0.1 k in [1, 2], nu = 6e-4, dt from CFL 0.5 of the initial field) in
+    float32 and in float64 on the same solver from the same float64 initial
+    field, compared every `--c3-every` steps up to `--c3-steps`: relative L2
+    of the state, the spectrum (largest shell difference relative to E, and
+    per shell over the resolved shells k <= N/3) and E, eps, P.  Prints one
+    JSON line."""
+    h3 = importlib.import_module("3dhit_b200")
+    N, total, every = args.size, args.c3_steps, args.c3_every
+    g64, g32 = h3.make_grid(N, dtype=torch.float64), h3.make_grid(N)
+    u64 = h3.hit_initial_field(0, g64)
+    dt = h3.cfl_dt(u64, g64, CFL)
+    u32 = u64.to(torch.complex64)
+    f = dict(eps=EPS, kmin=KMIN, kmax=KMAX)
+    p32 = h3.NSParams(nu=NU, forcing=h3.BandForcing(**f))
+    p64 = h3.NSParams(nu=NU, forcing=h3.BandForcing(**f))
+    r32, r64 = h3.make_ns_rhs(g32), h3.make_ns_rhs(g64)
+    kc = N // 3
+    rows, ms = [], {"f32": 0.0, "f64": 0.0}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    done = 0
+    while done < total:
+        n = min(every, total - done)
+        for key, (rhs, u, prm) in (("f32", (r32, u32, p32)), ("f64", (r64, u64, p64))):
+            e0.record()
+            out = h3.rollout(rhs, u, prm, dt, n, assume_dealiased=True)
+            e1.record()
+            torch.cuda.synchronize()
+            ms[key] += e0.elapsed_time(e1)
+            if key == "f32":
+                u32 = out
+            else:
+                u64 = out
+        done += n
+        state = float(torch.linalg.vector_norm(u32.to(torch.complex128) - u64) / torch.linalg.vector_norm(u64))
+        _, E32 = h3.energy_spectrum(u32, g32)
+        _, E64 = h3.energy_spectrum(u64, g64)
+        b32 = {k: float(v) for k, v in h3.energy_budget(u32, g32, NU, p32.forcing).items()}
+        b64 = {k: float(v) for k, v in h3.energy_budget(u64, g64, NU, p64.forcing).items()}
+        rows.append({"step": done, "t": done * dt, "state_rel_l2": state,
+                     "spectrum_max_abs_over_E": float(np.max(np.abs(E32 - E64)) / E64.sum()),
+                     "spectrum_max_rel_resolved": float(np.max(np.abs(E32 - E64)[:kc] / E64[:kc])),
+                     "budget_rel": {k: abs(b32[k] - b64[k]) / abs(b64[k]) for k in ("E", "eps", "P")},
+                     "E64": b64["E"], "eps64": b64["eps"]})
+        print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    h3.check_device("fp64 comparison")
+    line = {"check": f"config 3 precision: float32 vs float64 runs of the same solver, {N}^3 band-forced",
+            "grid": N, "steps": total, "dt": dt, "nu": NU, "forcing": "BandForcing eps=0.1 k=[1,2]",
+            "steps_per_s": {k: total / (v / 1000.0) for k, v in ms.items()}, "samples": rows,
+            "final": rows[-1]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def spectral_eddy_viscosity_les(data, steps, discard, coef=1.0, sample_every=50):
     """The coarse LES with a classical spectral closure instead of the MLP:
     the Chollet-Lesieur eddy viscosity nu_t(k) = coef C_K^(-3/2) (0.441 + 15.2
@@ -561,6 +616,10 @@ def main():
     ap.add_argument("--c2-steps", type=int, default=2000)
     ap.add_argument("--cufft-check", action="store_true",
                     help="cuFFT speed/correctness check of the transforms and the RHS (--size) instead of the benchmark")
+    ap.add_argument("--fp64-compare", action="store_true",
+                    help="config 3 precision statement: float32 vs float64 runs of the same solver (--size)")
+    ap.add_argument("--c3-steps", type=int, default=500)
+    ap.add_argument("--c3-every", type=int, default=100)
     ap.add_argument("--cl-fine", type=int, default=256)
     ap.add_argument("--cl-coarse", type=int, default=64)
     ap.add_argument("--cl-spinup", type=int, default=2000)
@@ -581,6 +640,8 @@ def main():
         return run_cufft_check(args)
     if args.config2:
         return run_config2(args)
+    if args.fp64_compare:
+        return run_fp64_compare(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -626,6 +687,7 @@ def main():
     barrier()
     ck = clocks.stop() if clocks else None
     ms_max = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    h3.check_device("bench timed rollout")  # no bounded wait of a transform pass gave up
     E_end = float(h3.energy(u, g))
     if not np.isfinite(E_end):
         raise RuntimeError("non-finite energy after the timed rollout")

@@ -123,6 +123,15 @@ int hit_rhs(hit_plan *plan, const void *u_hat, const hit_params *params,
  * Synchronises with the device.  No reference counterpart. */
 int hit_device_status(int *status);
 
+/* Test hook: the number of polls the tile/row-group waits of the TMA-staged
+ * transform passes make before giving up, on the current device (polls < 0
+ * restores the default of 2^22).  With 0 every such wait gives up at once:
+ * the CTA raises the flag hit_device_status reports, waits (with the default
+ * limit) for its copies in flight and ends, leaving its tiles untransformed.
+ * It lets a test exercise the give-up path without stalling the GPU.  No
+ * reference counterpart. */
+int hit_set_wait_limit(int polls);
+
 /* rhs and rollout with an external force f_ext (reference layout, device),
  * held constant over the call: rhs = project(dealias(u x w + forcing + f_ext))
  * - nu k^2 u, the RHS of a coarse LES whose subgrid-stress divergence is

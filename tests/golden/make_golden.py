@@ -15,8 +15,15 @@ numpy.fft (pocketfft) instead of jaxlib's ducc0, float32 reductions are
 NumPy's pairwise sums, and ``bincount`` accumulates in float64 before the cast
 to the weights' dtype.
 
-Usage (needs the reference checkout, so it runs only in the build container):
-    python tests/golden/make_golden.py [/path/to/reference]
+A second file, ``tests/golden/reference_aux.npz``, holds what the
+reference's driver-side code gives on the same inputs: the physical-space
+diagnostics (``velocity_samples``, ``velocity_moments``,
+``longitudinal_autocorrelation``, ``integral_lengthscale``), the steps at
+which its ``Callback`` / ``Diagnostic`` / ``FieldWriter`` schedules fire, and
+the steps at which ``evolve`` fires callbacks and prints progress.
+
+Usage (needs the reference checkout; pass its root, or set HIT3D_REFERENCE):
+    python tests/golden/make_golden.py /path/to/reference [--aux-only]
 """
 
 from __future__ import annotations
@@ -168,5 +175,77 @@ def main(ref_root):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)/1e6:.2f} MB")
 
 
+# schedule cases: (every_time, warmup_time, dt, t0, nsteps)
+SCHEDULES = [
+    (0.25, None, 1e-2, 0.0, 100), (0.5, 1.0, 0.1, 0.0, 30), (0.1, 0.0, 0.03, 0.0, 80),
+    (0.07, 0.2, 0.013, 0.05, 150), (1.0 / 3.0, 0.5, 1.0 / 30.0, 0.0, 120), (0.2, 0.0, 0.05, 1.0, 60),
+    (0.015, 0.0, 0.005, 0.0, 200), (0.3, 0.7, 0.1, 0.3, 40),
+]
+
+
+def aux(ref_root):
+    """Physical-space diagnostics, callback schedules and evolve firing steps
+    of the reference's own code (see the module docstring)."""
+    import contextlib
+    import io
+
+    ref = load_reference(ref_root)
+    G, NS, I, D, CB = ref.grid, ref.navierstokes, ref.integrators, ref.diagnostics, ref.callbacks
+    out = {}
+    for tag, dims, dt_, seed in (("c16f", (16, 16, 16), np.float32, 1), ("a16x32x8f", (16, 32, 8), np.float32, 4),
+                                 ("c16d", (16, 16, 16), np.float64, 3)):
+        og = orc.make_grid(*dims, dtype=dt_)
+        rg = G.make_grid(*dims, dtype=dt_)
+        u0 = orc.hit_initial_field(seed, og, k0=2.0 if min(dims) < 16 else 4.0)
+        out[f"{tag}/u0"] = u0
+        for c in range(3):
+            smp = np.asarray(D.velocity_samples(u0, rg, component=c))
+            out[f"{tag}/samples{c}"] = smp
+            mom = D.velocity_moments(smp)
+            out[f"{tag}/moments{c}"] = np.array([float(mom[k]) for k in ("mean", "variance", "skewness",
+                                                                          "flatness")])
+            r, f = D.longitudinal_autocorrelation(u0, rg, component=c)
+            out[f"{tag}/autocorr_r{c}"] = np.asarray(r)
+            out[f"{tag}/autocorr_f{c}"] = np.asarray(f)
+            out[f"{tag}/lengthscale{c}"] = np.array([D.integral_lengthscale(r, f)])
+    # schedules of the reference's wrappers
+    for i, (every_time, warm, dt, t0, n) in enumerate(SCHEDULES):
+        fw = CB.FieldWriter.__new__(CB.FieldWriter)  # is_due only: no file is made
+        fw.every, fw.every_time = 1, every_time
+        fw.warmup_time = 0.0 if warm is None else warm
+        cb = CB.Callback(lambda s: None, every_time=every_time)
+        out[f"sched{i}/case"] = np.array([every_time, -1.0 if warm is None else warm, dt, t0, n])
+        out[f"sched{i}/fieldwriter"] = np.array([k for k in range(n + 1) if fw.is_due(k, t0 + k * dt, dt)])
+        out[f"sched{i}/callback"] = np.array([k for k in range(n + 1) if cb.is_due(k, t0 + k * dt, dt)])
+    # evolve: which steps fire which callback, and which steps print progress
+    rg = G.make_grid(8, dtype=np.float64)
+    u0 = orc.hit_initial_field(0, orc.make_grid(8, dtype=np.float64), k0=2.0)
+    rhs = NS.make_ns_rhs(rg)
+    for j, (nsteps, dt, every, every_time, progress) in enumerate(
+            ((40, 0.03, 7, 0.25, 9), (25, 0.1, 4, 0.35, True), (13, 0.01, 5, None, False))):
+        seen = {"cb": [], "diag": []}
+        cbs = [CB.Callback(lambda s: seen["cb"].append(s.step), every_time=every_time) if every_time
+               else CB.Callback(lambda s: seen["cb"].append(s.step), every=every),
+               CB.Diagnostic(lambda s: (seen["diag"].append(s.step), 0.0)[1], every=every)]
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf):
+            I.evolve(rhs, u0, NS.NSParams(nu=0.05), rg, dt, nsteps, callbacks=cbs, progress=progress)
+        printed = [int(line.split()[1].split("/")[0]) for line in buf.getvalue().splitlines() if line.strip()]
+        out[f"evolve{j}/case"] = np.array([nsteps, dt, every, -1.0 if every_time is None else every_time,
+                                           -1.0 if progress is True else float(progress)])
+        out[f"evolve{j}/callback_steps"] = np.array(seen["cb"])
+        out[f"evolve{j}/diagnostic_steps"] = np.array(seen["diag"])
+        out[f"evolve{j}/progress_steps"] = np.array(printed)
+    path = os.path.join(HERE, "reference_aux.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)/1e6:.2f} MB")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else os.environ.get("HIT3D_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py /path/to/reference [--aux-only]  (or set HIT3D_REFERENCE)")
+    if "--aux-only" not in sys.argv:
+        main(root)
+    aux(root)

@@ -27,10 +27,19 @@ def _noalloc(nat, g, u):
     return E.cpu().numpy(), Ec.view(3, ns).cpu().numpy()
 
 
-@pytest.mark.parametrize("dims,dtype", [((64, 64, 64), torch.float32), ((32, 16, 64), torch.float64)])
-def test_noalloc_spectrum_matches_plan_entry_point(h3, dims, dtype):
+TWO_PI = 2 * np.pi
+
+
+# the last case is an anisotropic box (Ly = pi, Lz = 4 pi): the shell width
+# comes from Lx, ky and kz are scaled by their own lengths, and shells past
+# smax are dropped
+@pytest.mark.parametrize("dims,dtype,lengths", [((64, 64, 64), torch.float32, (TWO_PI,) * 3),
+                                                ((32, 16, 64), torch.float64, (TWO_PI,) * 3),
+                                                ((64, 32, 16), torch.float32, (TWO_PI, np.pi, 2 * TWO_PI))])
+def test_noalloc_spectrum_matches_plan_entry_point(h3, dims, dtype, lengths):
     nat = importlib.import_module("3dhit_b200._native")
-    g = h3.make_grid(*dims, dtype=dtype)
+    Lx, Ly, Lz = lengths
+    g = h3.make_grid(*dims, Lx=Lx, Ly=Ly, Lz=Lz, dtype=dtype)
     fields = [h3.random_field(3, g), h3.hit_initial_field(4, g) * 0.5]
     for u in fields:  # two calls in a row on the shared scratch
         E, Ec = _noalloc(nat, g, u)
