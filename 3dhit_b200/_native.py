@@ -14,7 +14,9 @@ import threading
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libhit3d_b200.so")
+# The in-tree build; HIT3D_LIB names another build of the same library (e.g.
+# one made with different compile options) to load instead.
+LIB_PATH = os.environ.get("HIT3D_LIB") or os.path.join(_HERE, "_lib", "libhit3d_b200.so")
 
 HIT_OK = 0
 HIT_E_INVALID = -1

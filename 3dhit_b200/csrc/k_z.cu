@@ -20,6 +20,7 @@
 #include "fft_core.cuh"
 #include "kernels.h"
 #include "tma.cuh"
+#include "zwarp.cuh"
 
 namespace hit {
 
@@ -210,6 +211,166 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
   cp_async_wait_all();
 }
 
+// k_zwarp: the fused z pass of k_zcross (same inputs, outputs and arithmetic
+// per value) with warp-resident transforms (zwarp.cuh), float32, H in {64,
+// 128, 256}.  Persistent CTAs of NWARP independent warps; warp g walks the row
+// groups g, g + (all warps), ...  A warp stages its group's 6 x ROWS input rows
+// (Mzp entries each) with bulk TMA copies issued by its lanes and counted on
+// its own mbarrier, and prefetches the next group as soon as the last input
+// field has passed through its first transform.  Per lane and row: the six
+// c2r transforms (pre-processing from the staged rows), u x w in registers as
+// the fields arrive (u first, then each w adds its terms), three r2c
+// transforms and the post-processing with the conjugate partner fetched by a
+// shuffle; outputs are written over the first three input fields of the row.
+
+constexpr int ZW_MINB = 3;  // CTAs per SM the register budget is sized for
+// DA: the dealiased layout, Mz = Nz/3 + 1 and Mzp = Mz rounded up to 8 as
+// compile-time constants, so the bounds of the pre-processing loads and of
+// the outputs fold into each value's position range (known-zero inputs are
+// not loaded, outputs past the row are not formed).
+template <int H> constexpr int zw_da_mz() { return (2 * H) / 3 + 1; }
+template <int H, int NWARP, bool DA>
+__global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float> a) {
+  using Z = ZW<H>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bars[NWARP];
+  float2* tws = reinterpret_cast<float2*>(smem_raw);
+  const int Mz = DA ? zw_da_mz<H>() : a.Mz;
+  const int Mzp = DA ? (zw_da_mz<H>() + 7) / 8 * 8 : a.Mzp;
+  // k < bound for a k known to lie in [lo, hi] (lo, hi compile-time)
+  auto below = [](int k, int lo, int hi, int bound) { return hi < bound ? true : (lo >= bound ? false : k < bound); };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = lane / Z::LPR, b = lane % Z::LPR;
+  const int stg_slots = 6 * Z::ROWS * Mzp;
+  float2* stg = tws + Z::TWS + warp * (stg_slots + Z::ROWS * Z::XS);  // [field][row][Mzp]
+  float2* xch = stg + stg_slots + q * Z::XS;
+  const float2* twz = tws + Z::TWZ;
+  zw_fill_twiddles<H, NWARP * 32>(tws, a.tw);
+  const uint32_t mb = tma::smem_u32(&bars[warp]);
+  if (lane == 0) tma::mbar_init(mb, 1);
+  tma::fence_async_smem();
+  __syncthreads();
+
+  const int wait_limit = g_z_wait_limit;
+  const long long ngroups = a.nrows / Z::ROWS;
+  const long long nwarps = (long long)gridDim.x * NWARP;
+  const uint32_t row_bytes = (uint32_t)(Mzp * sizeof(float2));
+  auto prefetch = [&](long long grp) {
+    if (lane == 0) tma::mbar_expect_tx(mb, 6u * Z::ROWS * row_bytes);
+    __syncwarp();
+    if (lane < 6 * Z::ROWS) {  // lane = field * ROWS + row
+      const int c = lane / Z::ROWS, rr = lane % Z::ROWS;
+      tma::load_bytes(stg + lane * Mzp, a.buf + c * a.c_stride + (grp * Z::ROWS + rr) * Mzp, row_bytes, mb);
+    }
+  };
+
+  pdl_wait();
+  pdl_trigger();
+  long long grp = (long long)blockIdx.x * NWARP + warp;
+  if (grp < ngroups) prefetch(grp);
+  uint32_t phase = 0;
+  const float s2 = 0.5f * a.scale * a.scale;  // both inverse normalisations and the r2c 1/2
+  for (; grp < ngroups; grp += nwarps) {
+    {
+      const bool ok = __all_sync(0xffffffffu, tma::mbar_wait(mb, phase, wait_limit));
+      phase ^= 1;
+      if (!ok) {
+        if (lane == 0) atomicExch(&g_z_timeout, 1);
+        tma::mbar_wait(mb, phase ^ 1, Z_WAIT);  // the copies in flight, once more with a limit
+        return;
+      }
+    }
+    float2 u0[8], u1[8], u2[8], n0[8], n1[8], n2[8];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      // c2r pre-processing of positions k = b + (H/8) r (see c2r_pre)
+      const float2* row = stg + (c * Z::ROWS + q) * Mzp;
+      float2 v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int k = b + Z::NB0 * r, kk = H - k;
+        float2 X = below(k, Z::NB0 * r, Z::NB0 * r + Z::NB0 - 1, Mz) ? row[k] : make_float2(0.f, 0.f);
+        float2 Y = below(kk, H - Z::NB0 * r - Z::NB0 + 1, H - Z::NB0 * r, Mz) ? row[kk] : make_float2(0.f, 0.f);
+        if (k == 0) {
+          X.y = 0.f;
+          Y.y = 0.f;
+        }
+        Y.y = -Y.y;
+        const float2 sm = cadd(X, Y), df = csub(X, Y);
+        float2 w = twz[k];
+        w.y = -w.y;
+        v[r] = cadd(sm, cmul_i(cmul(w, df)));
+      }
+      zw_transform<H, true>(v, xch, tws, b);
+      if (c == 5 && grp + nwarps < ngroups) prefetch(grp + nwarps);  // every lane is past its staged reads
+      // u x w (navierstokes.py:82-86) in the packed form of the real rows:
+      // n0 = u1 w2 - u2 w1, n1 = u2 w0 - u0 w2, n2 = u0 w1 - u1 w0
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const float2 x = v[r];
+        switch (c) {
+          case 0: u0[r] = x; break;
+          case 1: u1[r] = x; break;
+          case 2: u2[r] = x; break;
+          case 3:
+            n1[r] = __fmul2_rn(u2[r], x);
+            n2[r] = __fmul2_rn(u1[r], make_float2(-x.x, -x.y));
+            break;
+          case 4:
+            n0[r] = __fmul2_rn(u2[r], make_float2(-x.x, -x.y));
+            n2[r] = __ffma2_rn(u0[r], x, n2[r]);
+            break;
+          default:
+            n0[r] = __fmul2_rn(__ffma2_rn(u1[r], x, n0[r]), make_float2(s2, s2));
+            n1[r] = __fmul2_rn(__ffma2_rn(u0[r], make_float2(-x.x, -x.y), n1[r]), make_float2(s2, s2));
+            n2[r] = __fmul2_rn(n2[r], make_float2(s2, s2));
+            break;
+        }
+      }
+    }
+    // r2c of the three products; outputs over the first three input fields
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = c == 0 ? n0[r] : (c == 1 ? n1[r] : n2[r]);
+      zw_transform<H, false>(v, xch, tws, b);
+      float2* out = a.buf + c * a.c_stride + (grp * Z::ROWS + q) * Mzp;
+      const int partner = q * Z::LPR + ((Z::LPR - b) & (Z::LPR - 1));
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        // Z[H - k] of k = b + (H/8) r: lane (LPR - b) mod LPR of the row, value
+        // 7 - r; for b = 0 this lane's own value (8 - r) mod 8 (Z[H] = Z[0])
+        float2 t;
+        t.x = __shfl_sync(0xffffffffu, v[7 - r].x, partner);
+        t.y = __shfl_sync(0xffffffffu, v[7 - r].y, partner);
+        const float2 zb = b == 0 ? v[(8 - r) & 7] : t;
+        const int k = b + Z::NB0 * r;
+        if (below(k, Z::NB0 * r, Z::NB0 * r + Z::NB0 - 1, Mzp)) {
+          float2 x = make_float2(0.f, 0.f);
+          if (below(k, Z::NB0 * r, Z::NB0 * r + Z::NB0 - 1, Mz)) {  // r2c_post with the 1/2 folded into s2
+            float2 bc = zb;
+            bc.y = -bc.y;
+            const float2 E = cadd(v[r], bc), O = cmul_mi(csub(v[r], bc));
+            x = cadd(E, cmul(twz[k], O));
+          }
+          out[k] = x;
+        }
+      }
+      // bin H (general path: Mz = H + 1) and the row padding past it
+      if (!DA && b < Mzp - H) {
+        float2 x = make_float2(0.f, 0.f);
+        if (b == 0 && H < Mz) {
+          float2 bc = v[0];
+          bc.y = -bc.y;
+          x = cadd(cadd(v[0], bc), cmul(twz[H], cmul_mi(csub(v[0], bc))));
+        }
+        out[H + b] = x;
+      }
+    }
+  }
+}
+
 // Plain z c2r / r2c (to_physical / to_spectral).  Persistent CTAs walk the
 // (component, RB-row group) pairs; the rows of the next group are staged with
 // cp.async while the current group is transformed (a warp per row), as in
@@ -374,7 +535,54 @@ template <typename T, int HH, int RB, int NTZ, int MINB> cudaError_t launch_zcro
   return launch_pdl(k_zcross<T, HH, RB, NTZ, MINB>, nb, NTZ, smem, st, a);
 }
 
+// Warps per k_zwarp CTA.
+constexpr int ZW_WARPS = 4;
+
+template <int HH> size_t zwarp_smem(int Mzp) {
+  using Z = ZW<HH>;
+  return sizeof(float2) * (Z::TWS + (size_t)ZW_WARPS * (6 * Z::ROWS * Mzp + Z::ROWS * Z::XS));
+}
+
+template <int HH, bool DA> cudaError_t launch_zwarp_v(const ZCrossArgs<float>& a, cudaStream_t st) {
+  static PerDevice ready, cache;
+  // the opt-in covers the largest staging rows (Mzp = H + 8)
+  const size_t smax = zwarp_smem<HH>(HH + 8);
+  cudaError_t e = once_per_device(ready, [&] {
+    cudaError_t r = cudaFuncSetAttribute(k_zwarp<HH, ZW_WARPS, DA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smax);
+    if (r != cudaSuccess) return r;
+    return cudaFuncSetAttribute(k_zwarp<HH, ZW_WARPS, DA>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
+  });
+  if (e != cudaSuccess) return e;
+  const size_t smem = zwarp_smem<HH>(a.Mzp);
+  const long long groups = a.nrows / ZW<HH>::ROWS;
+  const int nb =
+      resident_grid(k_zwarp<HH, ZW_WARPS, DA>, ZW_WARPS * 32, smax, (groups + ZW_WARPS - 1) / ZW_WARPS, cache);
+  return launch_pdl(k_zwarp<HH, ZW_WARPS, DA>, nb, ZW_WARPS * 32, smem, st, a);
+}
+
+template <int HH> cudaError_t launch_zwarp(const ZCrossArgs<float>& a, cudaStream_t st) {
+  const bool da = a.Mz == zw_da_mz<HH>() && a.Mzp == (zw_da_mz<HH>() + 7) / 8 * 8;
+  return da ? launch_zwarp_v<HH, true>(a, st) : launch_zwarp_v<HH, false>(a, st);
+}
+
+// float32 rows of Nz = 128, 256, 512 (whole row groups, staging rows of at
+// most H + 8 entries) take the warp-resident kernel; every other case k_zcross.
+template <typename T> bool use_zwarp(int H, const ZCrossArgs<T>& a) {
+  if (!std::is_same<T, float>::value || !(H == 64 || H == 128 || H == 256)) return false;
+  const int rows = 256 / H;
+  return a.nrows % rows == 0 && a.Mzp % 8 == 0 && a.Mzp <= H + 8 && a.Mz <= a.Mzp;
+}
+
 template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, cudaStream_t st) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (use_zwarp(H, a)) {
+      if (H == 64) return launch_zwarp<64>(a, st);
+      if (H == 128) return launch_zwarp<128>(a, st);
+      return launch_zwarp<256>(a, st);
+    }
+  }
   return dispatch_half(H, [&](auto hh) {
     constexpr int HH = decltype(hh)::value;
     return launch_zcross_v<T, HH, z_rows_per_block<HH>(), z_threads<HH>(), 4>(a, st);

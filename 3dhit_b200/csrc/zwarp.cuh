@@ -1,0 +1,123 @@
+// Warp-resident transforms of the fused z pass (float32, H = Nz/2 in {64, 128,
+// 256}).
+//
+// A warp owns ROWS = 256/H whole (x, y) rows; LPR = H/8 lanes serve one row.
+// The half-length complex transform of a row (H points, see k_z.cu) runs on
+// the plan radix 8 -> R1 -> radix 8 (R1 = H/64; H = 64 has no middle stage):
+// every stage leaves each lane holding 8 complex values, the radix-8 stages
+// one butterfly per lane, the middle stage 8/R1 butterflies per lane.  Values
+// move between stages through a warp-private shared exchange buffer, laid out
+// so that every access of a half warp hits 16 distinct bank pairs (zw_slot),
+// and ordered by __syncwarp: no CTA barrier anywhere in the row loop.
+//
+// The first stage of the plan reads positions b + (H/8) r of the lane's row
+// (b = lane % LPR, r = 0..7) and the last stage writes positions b + (H/8) r,
+// so the inverse transforms leave each lane with the same 8 physical positions
+// of all six fields: the cross product u x w is formed in registers, and the
+// product is already laid out as the forward transform's first-stage input.
+// The r2c post-processing pairs Z[k] with Z[H-k], which sits in lane
+// (LPR - b) mod LPR of the same row: one __shfl_sync per value.
+#pragma once
+
+#include "fft_core.cuh"
+
+namespace hit {
+
+template <int H> struct ZW {
+  static_assert(H == 64 || H == 128 || H == 256, "warp-resident z rows need H in {64, 128, 256}");
+  static constexpr int LPR = H / 8;      // lanes per row
+  static constexpr int ROWS = 32 / LPR;  // rows per warp
+  static constexpr int R1 = H / 64;      // middle radix (1: no middle stage)
+  static constexpr int NB0 = H / 8;      // butterflies of a radix-8 stage
+  static constexpr int XS = H == 64 ? H + H / 8 : H + H / 16;  // exchange slots per row (see zw_slot)
+  // twiddle tables: middle stage (R1-1) x 8, last stage 7 x H/8, then
+  // exp(-2 pi i k / 2H) for k = 0..H (pre/post-processing of the real rows)
+  static constexpr int TW1 = 0;
+  static constexpr int TW2 = R1 > 1 ? (R1 - 1) * 8 : 0;
+  static constexpr int TWZ = TW2 + 7 * (H / 8);
+  static constexpr int TWS = (TWZ + H + 1 + 1) / 2 * 2;  // even: what follows stays 16-byte aligned
+};
+
+// Exchange slot of row position p: one pad slot after every 8 positions (H =
+// 64) or every 16 (H = 128, 256).  The accesses are, per half warp: the first
+// stage's stores of positions 8b + r (16 consecutive b), the middle stage's
+// loads of contiguous runs and stores of two runs of 8 positions, the last
+// stage's loads of contiguous runs.  An 8-byte slot s uses the bank pair of s
+// mod 16, and all of these accesses get 16 distinct pairs except the middle
+// stage's stores (two lanes per pair on half of them).  The padding is
+// additive in the fields of p that a lane's index and a value's index r fill,
+// so every access is the lane's base slot plus a constant offset.
+template <int H> __device__ __forceinline__ int zw_slot(int p) {
+  return H == 64 ? p + (p >> 3) : p + (p >> 4);
+}
+
+// Twiddle tables of ZW<H> from the global exp(-2 pi i m / TWN) table (all
+// threads of the CTA call; the caller synchronises before use).
+template <int H, int NTH> __device__ __forceinline__ void zw_fill_twiddles(float2* tws, const float2* __restrict__ tw) {
+  using Z = ZW<H>;
+  for (int e = threadIdx.x; e < Z::TWS; e += NTH) {
+    int m = 0;
+    if (e < Z::TW2) {  // middle stage: P = 8, radix R1: w_{8 R1}^{r k}
+      const int r = e / 8 + 1, k = e % 8;
+      m = r * k * (TWN / (8 * Z::R1));
+    } else if (e < Z::TWZ) {  // last stage: P = H/8, radix 8: w_H^{r k}
+      const int r = (e - Z::TW2) / Z::NB0 + 1, k = (e - Z::TW2) % Z::NB0;
+      m = r * k * (TWN / H);
+    } else if (e - Z::TWZ <= H) {
+      m = (e - Z::TWZ) * (TWN / (2 * H));
+    }
+    tws[e] = tw[m];
+  }
+}
+
+// The three stages of one H-point transform (INV: exp(+2 pi i nk/H)).  On
+// entry v[r] holds position b + (H/8) r of the lane's row, on exit output
+// b + (H/8) r.  xch is the row's exchange buffer; the warp must call this
+// converged.  Returns with the exchange buffer free for the next transform.
+template <int H, bool INV>
+__device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const float2* __restrict__ tws, int b) {
+  using Z = ZW<H>;
+  DFT<8, INV, float2>::run(v);  // stage 0 (P = 1): outputs 8b + r
+#pragma unroll
+  for (int r = 0; r < 8; ++r) xch[zw_slot<H>(8 * b + r)] = v[r];
+  __syncwarp();
+  if constexpr (Z::R1 > 1) {
+    constexpr int R1 = Z::R1, NB1 = H / R1, C1 = 8 / R1;
+    float2 u[C1][R1];
+#pragma unroll
+    for (int i = 0; i < C1; ++i) {
+      const int b1 = b + Z::LPR * i;
+#pragma unroll
+      for (int r = 0; r < R1; ++r) u[i][r] = xch[zw_slot<H>(b1 + NB1 * r)];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < C1; ++i) {
+      const int b1 = b + Z::LPR * i, k = b1 & 7;
+#pragma unroll
+      for (int r = 1; r < R1; ++r) {
+        float2 w = tws[Z::TW1 + (r - 1) * 8 + k];
+        if (INV) w.y = -w.y;
+        u[i][r] = cmul(u[i][r], w);
+      }
+      DFT<R1, INV, float2>::run(u[i]);
+      const int j = (b1 - k) * R1 + k;
+#pragma unroll
+      for (int r = 0; r < R1; ++r) xch[zw_slot<H>(j + 8 * r)] = u[i][r];
+    }
+    __syncwarp();
+  }
+  // last stage: radix 8, P = H/8, butterfly b (k = b, outputs b + (H/8) r)
+#pragma unroll
+  for (int r = 0; r < 8; ++r) v[r] = xch[zw_slot<H>(b + Z::NB0 * r)];
+  __syncwarp();
+#pragma unroll
+  for (int r = 1; r < 8; ++r) {
+    float2 w = tws[Z::TW2 + (r - 1) * Z::NB0 + b];
+    if (INV) w.y = -w.y;
+    v[r] = cmul(v[r], w);
+  }
+  DFT<8, INV, float2>::run(v);
+}
+
+}  // namespace hit
