@@ -164,61 +164,128 @@ cudaError_t launch_dealias_project(const V2<T>* in, V2<T>* out, const Geom& g, K
 }
 
 // ---------------------------------------------------------------------------
-// per-block spectral sums: shells (per component) and NSCAL scalars
+// per-block spectral sums: shells (per component) and NSCAL scalars,
+// compensated and in a fixed order (bit-identical from run to run)
 // ---------------------------------------------------------------------------
+struct KahanAcc {  // compensated running sum
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double x) {
+    const double y = x - c;
+    const double t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return s - c; }
+};
+
+constexpr int MS_WARPS = 4;  // warps per k_mode_sums block
+
+// A warp takes 32 consecutive kz modes of one (kx, ky) row at a time (the
+// chunks are dealt to the warps of the grid in a fixed order).  Along a row
+// |k| and hence the shell index never decrease with kz, so the lanes of one
+// shell form contiguous runs: a segmented shuffle scan in lane order gives
+// each run's sum in its last lane, which adds it (Kahan) to the warp's own
+// bins in shared memory; different runs have different shells, so no two
+// lanes touch one bin.  E, Omega and the band energy are per-lane Kahan sums.
+// At the end the warps' bins are added in warp order and the scalars by a
+// fixed shuffle tree, so the result does not depend on scheduling.
 template <typename T>
-__global__ void __launch_bounds__(NT) k_mode_sums(ModeSumArgs<T> a) {
+__global__ void __launch_bounds__(MS_WARPS * 32) k_mode_sums(ModeSumArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* bins = reinterpret_cast<double*>(smem_raw);  // [3][nshell]
-  __shared__ double red[32];
-  const Geom& g = a.g;
   const int nb3 = 3 * a.nshell;
-  for (int s = threadIdx.x; s < nb3; s += NT) bins[s] = 0.0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* bs = reinterpret_cast<double*>(smem_raw);  // [warp][nb3] sums, then [warp][nb3] compensations
+  double* bc = bs + MS_WARPS * nb3;
+  __shared__ double red[32];
+  for (int e = threadIdx.x; e < 2 * MS_WARPS * nb3; e += MS_WARPS * 32) bs[e] = 0.0;
   __syncthreads();
-  const long long nmodes = (long long)g.Mx * g.My * g.Mz;
-  double sE = 0, sO = 0, sB = 0;
-  for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < nmodes; m += (long long)gridDim.x * NT) {
-    const int k = (int)(m % g.Mz);
-    const long long r = m / g.Mz;
-    const int j = (int)(r % g.My), i = (int)(r / g.My);
+  const Geom& g = a.g;
+  const int nck = (g.Mz + 31) / 32;
+  const long long nchunks = (long long)g.Mx * g.My * nck;
+  double* wb = bs + warp * nb3;
+  double* wc = bc + warp * nb3;
+  KahanAcc sE, sO, sB;
+  for (long long ch = (long long)blockIdx.x * MS_WARPS + warp; ch < nchunks; ch += (long long)gridDim.x * MS_WARPS) {
+    const long long row = ch / nck;
+    const int k = (int)(ch % nck) * 32 + lane;
+    const int j = (int)(row % g.My), i = (int)(row / g.My);
+    const bool on = k < g.Mz;
     const int fx = full_pos(i, g.hx, g.Mx, g.Nx), fy = full_pos(j, g.hy, g.My, g.Ny);
-    const long long off = (long long)i * a.c_x + (long long)j * a.c_y + k;
-    double a2[3];
+    double e[3] = {0.0, 0.0, 0.0};
+    int s = 0x7fffffff;  // lanes past the row: a key no real shell has
+    if (on) {
+      const long long off = (long long)i * a.c_x + (long long)j * a.c_y + k;
+      const T k2 = k2_of(a.k.kx[fx], a.k.ky[fy], a.k.kz[k]);
+      const double w = herm_weight(g, k);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const V2<T> v = a.u[c * a.c_c + off];
-      a2[c] = (double)v.x * v.x + (double)v.y * v.y;
-    }
-    const T k2 = k2_of(a.k.kx[fx], a.k.ky[fy], a.k.kz[k]);
-    const double w = herm_weight(g, k);
-    const double t = a2[0] + a2[1] + a2[2];
-    sE += w * t;
-    sO += w * (double)k2 * t;
-    if (a.kmin2 <= k2 && k2 <= a.kmax2) sB += w * t;
-    if (a.nshell > 0) {
-      const int s = shell_of<T>(k2, a.k0);
-      if (s >= 0 && s < a.nshell) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          if (a2[c] != 0.0) atomicAdd(&bins[c * a.nshell + s], w * a2[c]);
+      for (int c = 0; c < 3; ++c) {
+        const V2<T> v = a.u[c * a.c_c + off];
+        e[c] = w * ((double)v.x * v.x + (double)v.y * v.y);
       }
+      const double t = (e[0] + e[1]) + e[2];
+      sE.add(t);
+      sO.add((double)k2 * t);
+      if (a.kmin2 <= k2 && k2 <= a.kmax2) sB.add(t);
+      if (a.nshell > 0) {
+        s = shell_of<T>(k2, a.k0);
+        if (s < 0 || s >= a.nshell) s = 0x7ffffffe;  // not binned (a key of its own)
+      }
+    }
+    if (a.nshell > 0) {
+      // segmented inclusive scan over runs of equal s (contiguous in lane order)
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int so = __shfl_up_sync(0xffffffffu, s, d);
+        double up[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) up[c] = __shfl_up_sync(0xffffffffu, e[c], d);
+        if (lane >= d && so == s) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) e[c] += up[c];
+        }
+      }
+      const int sn = __shfl_down_sync(0xffffffffu, s, 1);
+      if (on && s < a.nshell && (lane == 31 || sn != s)) {  // last lane of its run
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const int b = c * a.nshell + s;
+          const double y = e[c] - wc[b];
+          const double t = wb[b] + y;
+          wc[b] = (t - wb[b]) - y;
+          wb[b] = t;
+        }
+      }
+      __syncwarp();
     }
   }
   const int NV = nb3 + NSCAL;
   double* out = a.partial + (long long)blockIdx.x * NV;
-  double r = block_sum_f64(sE, red);
+  double r = block_sum_f64(sE.value(), red);
   if (threadIdx.x == 0) out[nb3 + 0] = r;
-  r = block_sum_f64(sO, red);
+  r = block_sum_f64(sO.value(), red);
   if (threadIdx.x == 0) out[nb3 + 1] = r;
-  r = block_sum_f64(sB, red);
+  r = block_sum_f64(sB.value(), red);
   if (threadIdx.x == 0) out[nb3 + 2] = r;
   __syncthreads();
-  for (int s = threadIdx.x; s < nb3; s += NT) out[s] = bins[s];
+  for (int b = threadIdx.x; b < nb3; b += MS_WARPS * 32) {
+    KahanAcc t;
+#pragma unroll
+    for (int w = 0; w < MS_WARPS; ++w) t.add(bs[w * nb3 + b] - bc[w * nb3 + b]);
+    out[b] = t.value();
+  }
+}
+
+template <typename T> size_t mode_sums_smem(int nshell) {
+  return sizeof(double) * 2 * MS_WARPS * 3 * (size_t)(nshell > 0 ? nshell : 1);
 }
 
 template <typename T> cudaError_t launch_mode_sums(const ModeSumArgs<T>& a, int nblocks, cudaStream_t st) {
-  const size_t smem = sizeof(double) * 3 * (a.nshell > 0 ? a.nshell : 1);
-  k_mode_sums<T><<<nblocks, NT, smem, st>>>(a);
+  const size_t smem = mode_sums_smem<T>(a.nshell);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_mode_sums<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_mode_sums<T><<<nblocks, MS_WARPS * 32, smem, st>>>(a);
   return cudaGetLastError();
 }
 

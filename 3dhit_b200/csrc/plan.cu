@@ -905,7 +905,16 @@ int hit_plan_create(int nx, int ny, int nz, double lx, double ly, double lz, int
   const int nmax = std::max(nx, std::max(ny, nz));
   p->smax = (int)std::ceil(std::sqrt(3.0) * nmax / 2.0) + 1;
   const long long nm = (long long)nx * ny * (nz / 2 + 1);
-  p->diag_blocks = (int)std::min<long long>((nm + NT - 1) / NT, 8 * 148);
+  {
+    // k_mode_sums: 4-warp blocks with per-warp compensated bins (2 x 4 x 3 x
+    // (smax + 1) doubles), as many resident per SM as their shared memory
+    // allows (at most 8), one resident wave
+    const long long bins_bytes = 2LL * 4 * 3 * (p->smax + 1) * 8;
+    const long long per_sm = std::max(1LL, std::min(8LL, (220LL * 1024) / (bins_bytes + 1024)));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+    p->diag_blocks = (int)std::min<long long>((nm + 127) / 128, per_sm * sms);
+  }
   int rc = dtype == HIT_DTYPE_F32 ? create_impl<float>(p) : create_impl<double>(p);
   if (rc == HIT_OK) {
     e = cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking);

@@ -471,6 +471,72 @@ def run_fp64_compare(args):
     return 0
 
 
+def run_kernel_rooflines(args):
+    """Roofline figures of the kernels outside the step: the spectral
+    reduction (shell spectra per component + E, Omega, band energy; one
+    read of the 3S-byte state) at --size^3, and the closure MLP on a batch of
+    64^3 x 16 points: inference (9 -> 64 -> 64 -> 64 -> 6, 18,304 flop and 60
+    bytes per point) and one training pass (forward, backward, weight
+    gradients).  Device times from CUDA events over 20 calls after 3 warm-up
+    calls; prints one JSON line."""
+    h3 = importlib.import_module("3dhit_b200")
+    cl = importlib.import_module("3dhit_b200.closure")
+    hbm, _ = peaks()
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            tflops = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        tflops = 1590.0
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    N = args.size
+    g = h3.make_grid(N)
+    u = h3.hit_initial_field(0, g)
+    ns = g.plan.num_shells
+    E = torch.empty(ns, dtype=torch.float64, device=g.device)
+    Ec = torch.empty(3 * ns, dtype=torch.float64, device=g.device)
+    nat = h3._native
+
+    def spectrum():
+        nat.call("hit_energy_spectrum", g.plan.handle, nat.ptr(u), nat.ptr(E), nat.ptr(Ec), nat.stream_ptr(g.device))
+
+    t_spec = timed(spectrum)
+    sbytes = 3 * spectral_bytes(N)
+    del u
+    P = 64 ** 3 * 16
+    torch.manual_seed(0)
+    model = cl.ClosureMLP(torch.device("cuda", 0))
+    x = torch.randn(P, cl.FEATURES, device="cuda")
+    tau = torch.randn(P, cl.OUTPUTS, device="cuda")
+    t_inf = timed(lambda: model.raw_forward(x))
+    t_train = timed(lambda: model.loss_and_grads(x, tau), reps=10)
+    model.check_errors()
+    h3.check_device("kernel rooflines")
+    fl = 2 * (9 * 64 + 64 * 64 + 64 * 64 + 64 * 6)
+    line = {"check": "roofline of the reductions and the closure MLP",
+            "spectrum": {"grid": N, "ms": t_spec, "alg_bytes": sbytes, "gbs": sbytes / t_spec / 1e6,
+                         "frac_hbm": sbytes / t_spec / 1e6 / hbm},
+            "mlp_inference": {"points": P, "ms": t_inf, "tflops": fl * P / t_inf / 1e9,
+                              "frac_bf16": fl * P / t_inf / 1e9 / tflops, "gbs": 60 * P / t_inf / 1e6,
+                              "frac_hbm": 60 * P / t_inf / 1e6 / hbm},
+            "mlp_training_pass": {"points": P, "ms": t_train, "tflops": 3 * fl * P / t_train / 1e9,
+                                  "frac_bf16": 3 * fl * P / t_train / 1e9 / tflops},
+            "peaks": {"hbm_gbs": hbm, "bf16_tflops": tflops}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def spectral_eddy_viscosity_les(data, steps, discard, coef=1.0, sample_every=50):
     """The coarse LES with a classical spectral closure instead of the MLP:
     the Chollet-Lesieur eddy viscosity nu_t(k) = coef C_K^(-3/2) (0.441 + 15.2
@@ -619,6 +685,8 @@ def main():
     ap.add_argument("--c2-steps", type=int, default=2000)
     ap.add_argument("--cufft-check", action="store_true",
                     help="cuFFT speed/correctness check of the transforms and the RHS (--size) instead of the benchmark")
+    ap.add_argument("--kernel-rooflines", action="store_true",
+                    help="roofline figures of the spectral reduction (--size) and the closure MLP kernels")
     ap.add_argument("--fp64-compare", action="store_true",
                     help="config 3 precision statement: float32 vs float64 runs of the same solver (--size)")
     ap.add_argument("--c3-steps", type=int, default=500)
@@ -645,6 +713,8 @@ def main():
         return run_config2(args)
     if args.fp64_compare:
         return run_fp64_compare(args)
+    if args.kernel_rooflines:
+        return run_kernel_rooflines(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
