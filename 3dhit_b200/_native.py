@@ -75,6 +75,10 @@ SIGNATURES = {
     "hit_rhs_forced": (_i, [_vp, _vp, _PP, _vp, _d, _vp, _vp]),
     "hit_device_status": (_i, [ctypes.POINTER(ctypes.c_int)]),
     "hit_set_wait_limit": (_i, [_i]),
+    "hit_rk4_step_forced_vjp": (_i, [_vp, _vp, _PP, _vp, _d, _d, _vp, _vp, _vp, _vp, _vp]),
+    "hit_sgs_force_vjp": (_i, [_vp, _vp, _vp, _vp]),
+    "hit_velocity_gradients_vjp": (_i, [_vp, _vp, _vp, _vp]),
+    "hit_mlp_vjp": (_i, [_vp, _vp, _vp, _i64, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hit_rollout_forced": (_i, [_vp, _vp, _PP, _vp, _d, _i64, _d, _vp, _vp]),
     "hit_profile_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _vp, _vp, _vp, _vp]),
     "hit_rhs_vjp": (_i, [_vp, _vp, _PP, _d, _vp, _vp, _vp, _vp]),

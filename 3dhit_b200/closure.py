@@ -85,12 +85,14 @@ class ClosureMLP:
         w4[:, :OUTPUTS] = self.W4
         b4 = torch.zeros(16, device=dev)
         b4[:OUTPUTS] = self.b4
-        keep = dict(
+        w1 = torch.zeros(16, 64, device=dev)  # backward layer 1 (input cotangents, `vjp`)
+        w1[:FEATURES] = self.W1
+        keep = dict(w1=w1.to(bf).contiguous(),
             w1t=w1t.to(bf).contiguous(), w2t=self.W2.T.to(bf).contiguous(), w3t=self.W3.T.to(bf).contiguous(),
             w4t=w4t.to(bf).contiguous(), w2=self.W2.to(bf).contiguous(), w3=self.W3.to(bf).contiguous(),
             w4=w4.to(bf).contiguous(), b2=self.b2.float().contiguous(), b3=self.b3.float().contiguous(),
             b4=b4.contiguous())
-        w = nat.MlpWeights(**{k: v.data_ptr() for k, v in keep.items()})
+        w = nat.MlpWeights(**{k: v.data_ptr() for k, v in keep.items() if k != "w1"})
         self._packed = (w, keep)
         return w
 
@@ -163,6 +165,36 @@ class ClosureMLP:
         self.W3.grad, self.b3.grad = dW3[:64].clone(), dW3[64].clone()
         self.W4.grad, self.b4.grad = dW4[:64, :OUTPUTS].clone(), dW4[64, :OUTPUTS].clone()
         return loss
+
+    def vjp(self, grads, ybar):
+        """Reverse-mode product through `forward_fields`: for the gradient
+        fields ``grads`` (9, P) and the cotangent ``ybar`` (6, P) of the
+        physical stress, returns the cotangent of ``grads`` (9, P) and those
+        of the master parameters (a list in the order of `params`), by the
+        tensor-core backward (``hit_mlp_vjp``).  P a multiple of 16."""
+        if getattr(self, "_physical", None) is None:
+            self.pack_physical()
+        w, keep = self._physical
+        P = grads.shape[1]
+        nbytes = nat.load().hit_mlp_workspace_bytes(P)
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        dev = self.device
+        dW1 = torch.empty(16, 64, device=dev)
+        dW2 = torch.empty(65, 64, device=dev)
+        dW3 = torch.empty(65, 64, device=dev)
+        dW4 = torch.empty(65, 16, device=dev)
+        xbar = torch.empty(FEATURES, P, device=dev)
+        grads = grads.contiguous()
+        ybar = ybar.to(torch.float32).contiguous()
+        nat.call("hit_mlp_vjp", ctypes_ref(w), keep["w1"].data_ptr(), nat.ptr(grads), P, 1, nat.ptr(ybar), P, 1, P,
+                 nat.ptr(self._ws), nat.ptr(dW1), nat.ptr(dW2), nat.ptr(dW3), nat.ptr(dW4), nat.ptr(xbar),
+                 nat.ptr(self._err), nat.stream_ptr(dev))
+        # the physical operands are W1 / x_scale and (W4, b4) * y_scale * sgs_scale
+        ys = self.y_scale * float(self.sgs_scale)
+        g = [dW1[:FEATURES] / self.x_scale[:, None], dW1[15].clone(), dW2[:64].clone(), dW2[64].clone(),
+             dW3[:64].clone(), dW3[64].clone(), dW4[:64, :OUTPUTS] * ys[None, :], dW4[64, :OUTPUTS] * ys]
+        return xbar, g
 
     def check_errors(self):
         if int(self._err.item()) != 0:

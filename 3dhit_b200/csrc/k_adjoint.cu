@@ -345,6 +345,76 @@ __global__ void __launch_bounds__(NT) k_sgs_force(const V2<T>* __restrict__ t, V
   }
 }
 
+// Transpose of k_sgs_force (the write form f = P(-1j K tau_hat), P the
+// dealias mask and projection, (K tau_hat)_i = k_j tau_hat_ij with the
+// symmetric tau in the order xx, yy, zz, xy, xz, yz).  Cotangents are
+// dL/dRe + i dL/dIm of each stored entry, so a per-mode complex-linear map
+// transposes to its conjugate transpose: g = P fbar (P is real symmetric per
+// mode), h = 1j g, tau_hat_bar = K^T h.  Written times scale / w (w the
+// Hermitian weight of the mode's plane): with scale = Nx Ny Nz the c2r of the
+// result is the cotangent of the physical stress, because the transpose of
+// rfftn is N^3 irfftn(. / w).
+template <typename T>
+__global__ void __launch_bounds__(NT) k_sgs_force_vjp(const V2<T>* __restrict__ fb, V2<T>* __restrict__ tb, Geom gm,
+                                                      KTab<T> kt, T scale) {
+  const long long nm = (long long)gm.Nx * gm.Ny * gm.Nzh;
+  for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < nm; m += (long long)gridDim.x * NT) {
+    int fx, fy, z;
+    const Mode<T> d = mode_of(m, gm, kt, fx, fy, z);
+    V2<T> h[3] = {fb[m], fb[nm + m], fb[2 * nm + m]};
+    proj_mask(d, h);
+    const T c = scale / (T)d.w;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) h[i] = cscale(cmul_i(h[i]), c);
+    tb[m] = cscale(h[0], d.kx);
+    tb[nm + m] = cscale(h[1], d.ky);
+    tb[2 * nm + m] = cscale(h[2], d.kz);
+    tb[3 * nm + m] = cadd(cscale(h[0], d.ky), cscale(h[1], d.kx));
+    tb[4 * nm + m] = cadd(cscale(h[0], d.kz), cscale(h[2], d.kx));
+    tb[5 * nm + m] = cadd(cscale(h[1], d.kz), cscale(h[2], d.ky));
+  }
+}
+
+// Transpose of the velocity gradients g_(3i+j) = irfftn(1j k_j u_hat_i): with
+// G the rfftn of the 9 physical gradient cotangents, u_bar_i += sum_j
+// (-1j k_j) (w / N^3) G_ij (the transpose of irfftn is w rfftn(.) / N^3).
+template <typename T>
+__global__ void __launch_bounds__(NT) k_grad9_vjp(const V2<T>* __restrict__ G, V2<T>* __restrict__ ub, Geom gm,
+                                                  KTab<T> kt, T inv_n3) {
+  const long long nm = (long long)gm.Nx * gm.Ny * gm.Nzh;
+  for (long long m = blockIdx.x * (long long)NT + threadIdx.x; m < nm; m += (long long)gridDim.x * NT) {
+    const int z = (int)(m % gm.Nzh);
+    const long long r = m / gm.Nzh;
+    const int fy = (int)(r % gm.Ny), fx = (int)(r / gm.Ny);
+    const T k[3] = {kt.kx[fx], kt.ky[fy], kt.kz[z]};
+    const T c = (T)herm_weight(gm, z) * inv_n3;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      V2<T> s = czero<T>();
+#pragma unroll
+      for (int j = 0; j < 3; ++j) s = cadd(s, cscale(G[(3 * i + j) * nm + m], k[j]));
+      ub[i * nm + m] = cadd(ub[i * nm + m], cscale(cmul_mi(s), c));
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_sgs_force_vjp(const V2<T>* fb, V2<T>* tb, const Geom& gm, KTab<T> kt, T scale, cudaStream_t st) {
+  k_sgs_force_vjp<T><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(fb, tb, gm, kt, scale);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_grad9_vjp(const V2<T>* G, V2<T>* ub, const Geom& gm, KTab<T> kt, T inv_n3, cudaStream_t st) {
+  k_grad9_vjp<T><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(G, ub, gm, kt, inv_n3);
+  return cudaGetLastError();
+}
+template cudaError_t launch_sgs_force_vjp<float>(const float2*, float2*, const Geom&, KTab<float>, float, cudaStream_t);
+template cudaError_t launch_sgs_force_vjp<double>(const double2*, double2*, const Geom&, KTab<double>, double,
+                                                  cudaStream_t);
+template cudaError_t launch_grad9_vjp<float>(const float2*, float2*, const Geom&, KTab<float>, float, cudaStream_t);
+template cudaError_t launch_grad9_vjp<double>(const double2*, double2*, const Geom&, KTab<double>, double,
+                                              cudaStream_t);
+
 template <typename T> cudaError_t launch_grad9(const V2<T>* u, V2<T>* g, const Geom& gm, KTab<T> kt, cudaStream_t st) {
   k_grad9<T><<<grid_of((long long)gm.Nx * gm.Ny * gm.Nzh), NT, 0, st>>>(u, g, gm, kt);
   return cudaGetLastError();

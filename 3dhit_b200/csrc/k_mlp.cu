@@ -79,6 +79,7 @@ template <bool TRAIN> struct MlpSmem {
   unsigned char w1t[64 * 16 * 2], w2t[64 * 64 * 2], w3t[64 * 64 * 2], w4t[16 * 64 * 2];
   // backward operands (training only)
   unsigned char w4[TRAIN ? 64 * 16 * 2 : 16], w3[TRAIN ? 64 * 64 * 2 : 16], w2[TRAIN ? 64 * 64 * 2 : 16];
+  unsigned char w1[TRAIN ? 16 * 64 * 2 : 16];  // backward layer 1 (input gradient, vector-Jacobian mode)
   unsigned char x0[128 * 16 * 2];                   // a0, later dz4
   unsigned char buf[TRAIN ? 2 : 1][128 * 64 * 2];  // activations / gradients (ping-pong when training)
   float b2[64], b3[64], b4[16];
@@ -108,6 +109,7 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
     load_kmajor(S.w4, a.w4, 64, 16);
     load_kmajor(S.w3, a.w3, 64, 64);
     load_kmajor(S.w2, a.w2, 64, 64);
+    if (a.xbar) load_kmajor(S.w1, a.w1, 16, 64);
   }
   for (int i = tid; i < 64; i += 128) {
     S.b2[i] = a.b2[i];
@@ -223,7 +225,10 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
       float dz[16];
   #pragma unroll
       for (int i = 0; i < 16; ++i) dz[i] = 0.f;
-      if (in) {
+      if (in && a.ybar) {  // vector-Jacobian mode: the upstream dL/dy
+  #pragma unroll
+        for (int i = 0; i < 6; ++i) dz[i] = a.ybar[i * a.yb_sf + p * a.yb_sp];
+      } else if (in) {
   #pragma unroll
         for (int i = 0; i < 6; ++i) {
           const float r = y[i] - a.tau[p * 6 + i];
@@ -254,7 +259,16 @@ __global__ void __launch_bounds__(128) k_mlp(MlpArgs a) {
       mma(192, S.buf[1], 64, S.w3, 64, 4, id64);  // da2 = dz3 W3^T
       back(64, S.buf[0], a.dzT2, S.b2);
       mma(192, S.buf[0], 64, S.w2, 64, 4, id64);  // da1 = dz2 W2^T
-      back(0, nullptr, a.dzT1, nullptr);
+      back(0, a.xbar ? S.buf[1] : nullptr, a.dzT1, nullptr);
+      if (a.xbar) {  // dx = dz1 W1 (TMEM columns 0..15, free once z1 is read)
+        mma(0, S.buf[1], 64, S.w1, 64, 4, id16);
+        float dx[16];
+        tc::tmem_ld16(lane_base, dx);
+        if (in) {
+  #pragma unroll
+          for (int i = 0; i < 9; ++i) a.xbar[i * a.x_sf + p * a.x_sp] = dx[i];
+        }
+      }
     }
   }
   if (!ok && tid == 0) atomicExch(a.err, 1);

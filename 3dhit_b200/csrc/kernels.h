@@ -253,6 +253,10 @@ cudaError_t launch_axpby(const V2<T>* x, T alpha, const V2<T>* y, T beta, V2<T>*
 template <typename T> cudaError_t launch_grad9(const V2<T>* u, V2<T>* g, const Geom& gm, KTab<T> kt, cudaStream_t st);
 template <typename T>
 cudaError_t launch_sgs_force(const V2<T>* t, V2<T>* du, const Geom& gm, KTab<T> kt, cudaStream_t st, bool add);
+template <typename T>
+cudaError_t launch_sgs_force_vjp(const V2<T>* fb, V2<T>* tb, const Geom& gm, KTab<T> kt, T scale, cudaStream_t st);
+template <typename T>
+cudaError_t launch_grad9_vjp(const V2<T>* G, V2<T>* ub, const Geom& gm, KTab<T> kt, T inv_n3, cudaStream_t st);
 
 cudaError_t launch_tcgemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M,
                           int N, int K, int* err, cudaStream_t st, int splits = 1, float* work = nullptr);
@@ -272,6 +276,14 @@ struct MlpArgs {
   __nv_bfloat16 *dzT1, *dzT2, *dzT3, *dzT4;  // [64|64|64|16][P]
   double* loss;      // [grid] partial sums of (y - tau)^2
   int* err;
+  // vector-Jacobian mode (training instantiation): with ybar set, dL/dy of
+  // point p, component c is ybar[c * yb_sf + p * yb_sp] (instead of the MSE
+  // gradient of tau); with xbar set (and w1, the backward layer-1 weight W1
+  // [16][64], rows 0-8 used), dL/dx of feature f goes to xbar[f * x_sf + p * x_sp]
+  const float* ybar;
+  long long yb_sf, yb_sp;
+  float* xbar;
+  const __nv_bfloat16* w1;
 };
 size_t mlp_smem_bytes();
 cudaError_t launch_mlp(const MlpArgs& a, int grid, cudaStream_t st);

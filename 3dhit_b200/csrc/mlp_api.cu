@@ -52,6 +52,54 @@ MlpArgs args_of(const hit_mlp_weights* w) {
 }
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// One fused k_mlp pass over P points (forward, output cotangent, backward
+// through the layers; a.tau or a.ybar set) and the four weight-gradient GEMMs
+// dW_l = a_{l-1}^T dz_l; loss (nullable) receives the MSE loss.
+int run_grads(MlpArgs a, int64_t P, void* ws, float* dW1, float* dW2, float* dW3, float* dW4, double* loss, int* err,
+              cudaStream_t st, const char* who) {
+  if (P < 16 || P % 16) return hit::record_error(HIT_E_INVALID, std::string(who) + ": P must be a positive multiple of 16");
+  if (P > (int64_t)1 << 30) return hit::record_error(HIT_E_UNSUPPORTED, std::string(who) + ": P too large");
+  a.P = P;
+  a.inv_count = (float)(1.0 / ((double)P * 6.0));
+  a.err = err;
+  __nv_bfloat16* b = static_cast<__nv_bfloat16*>(ws);
+  auto take = [&](int rows) {
+    __nv_bfloat16* r = b;
+    b += (size_t)rows * P;
+    return r;
+  };
+  a.aT0 = take(16);
+  a.aT1 = take(65);
+  a.aT2 = take(65);
+  a.aT3 = take(65);
+  a.dzT1 = take(64);
+  a.dzT2 = take(64);
+  a.dzT3 = take(64);
+  a.dzT4 = take(16);
+  unsigned char* rest = static_cast<unsigned char*>(ws) + align256((size_t)ROWS * P * 2);
+  float* work = reinterpret_cast<float*>(rest);
+  double* part = reinterpret_cast<double*>(rest + align256((size_t)GRAD_SPLITS * 65 * 64 * 4));
+  a.loss = part;
+  const int grid = (int)std::min<int64_t>((P + 127) / 128, MLP_GRID);
+  cudaError_t e = hit::launch_mlp(a, grid, st);
+  if (e != cudaSuccess) return cuda_err(e, who);
+  const int K = (int)P, splits = (int)std::min<int64_t>(GRAD_SPLITS, P / 16);
+  struct G {
+    const __nv_bfloat16 *A, *B;
+    float* C;
+    int M, N;
+  } gs[4] = {{a.aT3, a.dzT4, dW4, 65, 16}, {a.aT2, a.dzT3, dW3, 65, 64}, {a.aT1, a.dzT2, dW2, 65, 64},
+             {a.aT0, a.dzT1, dW1, 16, 64}};
+  for (const G& g : gs) {
+    e = hit::launch_tcgemm(g.A, K, g.B, K, g.C, g.N, g.M, g.N, K, err, st, splits, work);
+    if (e != cudaSuccess) return cuda_err(e, who);
+  }
+  if (!loss) return HIT_OK;
+  k_loss<<<1, 32, 0, st>>>(part, grid, 1.0 / ((double)P * 6.0), loss);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? HIT_OK : cuda_err(e, who);
+}
 }  // namespace
 
 extern "C" {
@@ -89,52 +137,30 @@ int hit_mlp_train_grads(const hit_mlp_weights* w, const float* x, const float* t
                         float* dW2, float* dW3, float* dW4, double* loss, int* err, void* stream) {
   if (!weights_ok(w, true) || !x || !tau || !ws || !dW1 || !dW2 || !dW3 || !dW4 || !loss || !err)
     return hit::record_error(HIT_E_INVALID, "mlp_train_grads: NULL argument");
-  if (P < 16 || P % 16) return hit::record_error(HIT_E_INVALID, "mlp_train_grads: P must be a positive multiple of 16");
-  if (P > (int64_t)1 << 30) return hit::record_error(HIT_E_UNSUPPORTED, "mlp_train_grads: P too large");
-  cudaStream_t st = (cudaStream_t)stream;
   MlpArgs a = args_of(w);
   a.x = x;
   a.x_sf = 1;
   a.x_sp = 9;
   a.tau = tau;
-  a.P = P;
-  a.inv_count = (float)(1.0 / ((double)P * 6.0));
-  a.err = err;
-  __nv_bfloat16* b = static_cast<__nv_bfloat16*>(ws);
-  auto take = [&](int rows) {
-    __nv_bfloat16* r = b;
-    b += (size_t)rows * P;
-    return r;
-  };
-  a.aT0 = take(16);
-  a.aT1 = take(65);
-  a.aT2 = take(65);
-  a.aT3 = take(65);
-  a.dzT1 = take(64);
-  a.dzT2 = take(64);
-  a.dzT3 = take(64);
-  a.dzT4 = take(16);
-  unsigned char* rest = static_cast<unsigned char*>(ws) + align256((size_t)ROWS * P * 2);
-  float* work = reinterpret_cast<float*>(rest);
-  double* part = reinterpret_cast<double*>(rest + align256((size_t)GRAD_SPLITS * 65 * 64 * 4));
-  a.loss = part;
-  const int grid = (int)std::min<int64_t>((P + 127) / 128, MLP_GRID);
-  cudaError_t e = hit::launch_mlp(a, grid, st);
-  if (e != cudaSuccess) return cuda_err(e, "mlp_train_grads (pass)");
-  const int K = (int)P, splits = (int)std::min<int64_t>(GRAD_SPLITS, P / 16);
-  struct G {
-    const __nv_bfloat16 *A, *B;
-    float* C;
-    int M, N;
-  } gs[4] = {{a.aT3, a.dzT4, dW4, 65, 16}, {a.aT2, a.dzT3, dW3, 65, 64}, {a.aT1, a.dzT2, dW2, 65, 64},
-             {a.aT0, a.dzT1, dW1, 16, 64}};
-  for (const G& g : gs) {
-    e = hit::launch_tcgemm(g.A, K, g.B, K, g.C, g.N, g.M, g.N, K, err, st, splits, work);
-    if (e != cudaSuccess) return cuda_err(e, "mlp_train_grads (weight gradients)");
-  }
-  k_loss<<<1, 32, 0, st>>>(part, grid, 1.0 / ((double)P * 6.0), loss);
-  e = cudaGetLastError();
-  return e == cudaSuccess ? HIT_OK : cuda_err(e, "mlp_train_grads (loss)");
+  return run_grads(a, P, ws, dW1, dW2, dW3, dW4, loss, err, (cudaStream_t)stream, "mlp_train_grads");
+}
+
+int hit_mlp_vjp(const hit_mlp_weights* w, const void* w1, const float* x, int64_t x_sf, int64_t x_sp,
+                const float* ybar, int64_t y_sf, int64_t y_sp, int64_t P, void* ws, float* dW1, float* dW2,
+                float* dW3, float* dW4, float* xbar, int* err, void* stream) {
+  if (!weights_ok(w, true) || !x || !ybar || !ws || !dW1 || !dW2 || !dW3 || !dW4 || !err || (xbar && !w1))
+    return hit::record_error(HIT_E_INVALID, "mlp_vjp: NULL argument");
+  MlpArgs a = args_of(w);
+  a.x = x;
+  a.x_sf = x_sf;
+  a.x_sp = x_sp;
+  a.tau = ybar;  // selects the training instantiation; the cotangent replaces the loss gradient
+  a.ybar = ybar;
+  a.yb_sf = y_sf;
+  a.yb_sp = y_sp;
+  a.xbar = xbar;
+  a.w1 = static_cast<const __nv_bfloat16*>(w1);
+  return run_grads(a, P, ws, dW1, dW2, dW3, dW4, nullptr, err, (cudaStream_t)stream, "mlp_vjp");
 }
 
 }  // extern "C"

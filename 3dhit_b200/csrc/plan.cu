@@ -142,7 +142,7 @@ struct hit_plan {
   // adjoint workspace (reference layout): transform inputs/outputs of the RHS
   // transpose, its float64 sums and scalars, the RK4 stage inputs and
   // cotangents, and the rollout checkpoints
-  Buf ax9, aph, as6, apart, asums, ascal, apct, ast[3], ak, akb, asb, aacc, aub, ack, aseg;
+  Buf ax9, aph, as6, apart, asums, ascal, apct, ast[3], ak, akb, asb, aacc, aub, ack, aseg, afb;
   cudaStream_t cap = nullptr;  // private stream used only for graph capture
 };
 
@@ -732,9 +732,13 @@ hit_params general_params(const hit_params* pr) {
 
 // ub_out = (d rk4_step / d u)^T ub_in at u (stage inputs recomputed); ub_out
 // may alias ub_in.
+// With fext (reference layout) the step holds that force over its four
+// stages (rk4_step(..., f_ext=), the LES step), and fbar (nullable) receives
+// the force's cotangent: every stage adds P f (P = dealias + projection), so
+// fbar = P (sum of the stages' cotangents).
 template <typename T>
 int rk4_vjp_impl(hit_plan* p, const V2<T>* u, const hit_params* pr, double dt, const V2<T>* ub_in, V2<T>* ub_out,
-                 double* pct, cudaStream_t st) {
+                 double* pct, cudaStream_t st, const void* fext = nullptr, V2<T>* fbar = nullptr) {
   const long long n = 3LL * p->Nx * p->Ny * (p->Nz / 2 + 1);
   const size_t bytes = n * sizeof(V2<T>);
   int rc;
@@ -750,26 +754,44 @@ int rk4_vjp_impl(hit_plan* p, const V2<T>* u, const hit_params* pr, double dt, c
   V2<T>* SB = vp<T>(p->asb);
   V2<T>* ACC = vp<T>(p->aacc);
   const T h = (T)(0.5 * dt), d = (T)dt, d3 = (T)(dt / 3.0), d6 = (T)(dt / 6.0);
+  V2<T>* FB = nullptr;
+  if (fbar) {
+    if ((rc = ensure(p->afb, bytes))) return rc;
+    FB = vp<T>(p->afb);
+  }
+  // the stages' cotangents summed into FB (first one: FB = KB)
+  auto add_fb = [&](bool first) -> int {
+    if (FB) HIT_CK(launch_axpby<T>(KB, T(1), first ? nullptr : FB, first ? T(0) : T(1), FB, n, st));
+    return HIT_OK;
+  };
   // stage inputs (integrators.py:32-38)
-  if ((rc = rhs_impl<T>(p, u, &pg, K, nullptr, st))) return rc;
+  if ((rc = rhs_impl<T>(p, u, &pg, K, fext, st))) return rc;
   HIT_CK(launch_axpby<T>(u, T(1), K, h, S2, n, st));
-  if ((rc = rhs_impl<T>(p, S2, &pg, K, nullptr, st))) return rc;
+  if ((rc = rhs_impl<T>(p, S2, &pg, K, fext, st))) return rc;
   HIT_CK(launch_axpby<T>(u, T(1), K, h, S3, n, st));
-  if ((rc = rhs_impl<T>(p, S3, &pg, K, nullptr, st))) return rc;
+  if ((rc = rhs_impl<T>(p, S3, &pg, K, fext, st))) return rc;
   HIT_CK(launch_axpby<T>(u, T(1), K, d, S4, n, st));
   // transpose of u + dt/6 (k1 + 2 k2 + 2 k3 + k4), stage by stage backwards
   HIT_CK(launch_axpby<T>(ub_in, d6, nullptr, T(0), KB, n, st));
+  if ((rc = add_fb(true))) return rc;
   if ((rc = rhs_vjp_impl<T>(p, S4, s, KB, SB, pct, st))) return rc;
   HIT_CK(launch_axpby<T>(ub_in, T(1), SB, T(1), ACC, n, st));
   HIT_CK(launch_axpby<T>(ub_in, d3, SB, d, KB, n, st));
+  if ((rc = add_fb(false))) return rc;
   if ((rc = rhs_vjp_impl<T>(p, S3, s, KB, SB, pct, st))) return rc;
   HIT_CK(launch_axpby<T>(ACC, T(1), SB, T(1), ACC, n, st));
   HIT_CK(launch_axpby<T>(ub_in, d3, SB, h, KB, n, st));
+  if ((rc = add_fb(false))) return rc;
   if ((rc = rhs_vjp_impl<T>(p, S2, s, KB, SB, pct, st))) return rc;
   HIT_CK(launch_axpby<T>(ACC, T(1), SB, T(1), ACC, n, st));
   HIT_CK(launch_axpby<T>(ub_in, d6, SB, h, KB, n, st));
+  if ((rc = add_fb(false))) return rc;
   if ((rc = rhs_vjp_impl<T>(p, u, s, KB, SB, pct, st))) return rc;
   HIT_CK(launch_axpby<T>(ACC, T(1), SB, T(1), ub_out, n, st));
+  if (fbar) {
+    const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+    HIT_CK(launch_dealias_project<T>(FB, fbar, g, ktab_of<T>(p), 1, 1, st));
+  }
   return HIT_OK;
 }
 
@@ -826,6 +848,42 @@ int vjp_entry(hit_plan* p, int which, const void* u, const hit_params* pr, doubl
   else rc = rollout_vjp_impl<T>(p, u, pr, dt, nsteps, K, ct, ubar, pct, st);
   if (rc) return rc;
   if (pct_out) HIT_CK(cudaMemcpyAsync(pct_out, pct, 3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return HIT_OK;
+}
+
+template <typename T>
+int forced_vjp_entry(hit_plan* p, const void* u, const hit_params* pr, const void* f, double dt, const void* ct,
+                     void* ubar, void* fbar, double* pct_out, cudaStream_t st) {
+  int rc;
+  if ((rc = ensure(p->apct, 4 * sizeof(double)))) return rc;
+  double* pct = static_cast<double*>(p->apct.p);
+  HIT_CK(cudaMemsetAsync(pct, 0, 4 * sizeof(double), st));
+  if ((rc = rk4_vjp_impl<T>(p, static_cast<const V2<T>*>(u), pr, dt, static_cast<const V2<T>*>(ct),
+                            static_cast<V2<T>*>(ubar), pct, st, f, static_cast<V2<T>*>(fbar))))
+    return rc;
+  if (pct_out) HIT_CK(cudaMemcpyAsync(pct_out, pct, 3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return HIT_OK;
+}
+
+// tau_bar (physical, 6 x N^3) = cotangent of the stress whose sgs force has
+// cotangent f_bar (transposes of hit_sgs_force and of the stress's rfftn)
+template <typename T> int sgs_force_vjp_impl(hit_plan* p, const void* fbar, void* tbar, cudaStream_t st) {
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  int rc;
+  if ((rc = ensure(p->ax9, 9 * (size_t)g.Nx * g.Ny * g.Nzh * sizeof(V2<T>)))) return rc;
+  HIT_CK(launch_sgs_force_vjp<T>(static_cast<const V2<T>*>(fbar), vp<T>(p->ax9), g, ktab_of<T>(p),
+                                 (T)((double)p->Nx * p->Ny * p->Nz), st));
+  return to_physical_impl<T>(p, p->ax9.p, 6, tbar, st);
+}
+
+// u_bar += cotangent of u_hat whose velocity gradients have cotangent g_bar
+template <typename T> int grad_vjp_impl(hit_plan* p, const void* gbar, void* ubar, cudaStream_t st) {
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  int rc;
+  if ((rc = ensure(p->ax9, 9 * (size_t)g.Nx * g.Ny * g.Nzh * sizeof(V2<T>)))) return rc;
+  if ((rc = to_spectral_impl<T>(p, gbar, 9, p->ax9.p, st))) return rc;
+  HIT_CK(launch_grad9_vjp<T>(vp<T>(p->ax9), static_cast<V2<T>*>(ubar), g, ktab_of<T>(p),
+                             (T)(1.0 / ((double)p->Nx * p->Ny * p->Nz)), st));
   return HIT_OK;
 }
 
@@ -949,7 +1007,7 @@ int hit_plan_destroy(hit_plan* p) {
   release(p->dpartial);
   release(p->dsums);
   for (Buf* b : {&p->ax9, &p->aph, &p->as6, &p->apart, &p->asums, &p->ascal, &p->apct, &p->ast[0], &p->ast[1],
-                 &p->ast[2], &p->ak, &p->akb, &p->asb, &p->aacc, &p->aub, &p->ack, &p->aseg})
+                 &p->ast[2], &p->ak, &p->akb, &p->asb, &p->aacc, &p->aub, &p->ack, &p->aseg, &p->afb})
     release(*b);
   if (p->cap) cudaStreamDestroy(p->cap);
   delete p;
@@ -1109,6 +1167,30 @@ int hit_rk4_step_vjp(hit_plan* p, const void* u_hat, const hit_params* pr, doubl
     return fail(HIT_E_UNSUPPORTED, "the integrating-factor RK4 step has no transpose");
   DeviceGuard dg(p->device);
   return DISPATCH(p, vjp_entry)(p, 1, u_hat, pr, dt, 1, 1, ct, u_bar, param_ct, (cudaStream_t)stream);
+}
+
+int hit_rk4_step_forced_vjp(hit_plan* p, const void* u_hat, const hit_params* pr, const void* f_ext, double dt,
+                            double t, const void* ct, void* u_bar, void* f_bar, double* param_ct, void* stream) {
+  (void)t;
+  if (!p || !u_hat || !f_ext || !ct || !u_bar) return fail(HIT_E_INVALID, "NULL argument");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  if (pr->flags & HIT_FLAG_INTEGRATING_FACTOR)
+    return fail(HIT_E_UNSUPPORTED, "the integrating-factor RK4 step has no transpose");
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, forced_vjp_entry)(p, u_hat, pr, f_ext, dt, ct, u_bar, f_bar, param_ct, (cudaStream_t)stream);
+}
+
+int hit_sgs_force_vjp(hit_plan* p, const void* f_bar, void* tau_bar, void* stream) {
+  if (!p || !f_bar || !tau_bar) return fail(HIT_E_INVALID, "NULL argument");
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, sgs_force_vjp_impl)(p, f_bar, tau_bar, (cudaStream_t)stream);
+}
+
+int hit_velocity_gradients_vjp(hit_plan* p, const void* grads_bar, void* u_bar, void* stream) {
+  if (!p || !grads_bar || !u_bar) return fail(HIT_E_INVALID, "NULL argument");
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, grad_vjp_impl)(p, grads_bar, u_bar, (cudaStream_t)stream);
 }
 
 int hit_rollout_vjp(hit_plan* p, const void* u0, const hit_params* pr, double dt, int64_t nsteps, double t0,

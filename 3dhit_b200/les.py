@@ -36,7 +36,7 @@ from .integrators import rk4_step, rollout
 from .navierstokes import NSParams, make_ns_rhs
 
 __all__ = ["box_filter", "velocity_gradients", "sgs_stress", "LESRHS", "FusedLESStep", "make_dataset", "train",
-           "run_les"]
+           "run_les", "spectrum_log_loss", "les_window_grad", "train_a_posteriori"]
 
 _PAIRS = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
 
@@ -223,7 +223,7 @@ def make_dataset(fine_n=256, coarse_n=64, nu=1.5e-3, E_target=1.5, spinup=2000, 
     Pc = coarse.Nx * coarse.Ny * coarse.Nz
     X = torch.empty(snapshots, 9, Pc, device=device)
     Y = torch.empty(snapshots, 6, Pc, device=device)
-    spectra, A, E_f = [], [], []
+    spectra, A, E_f, U = [], [], [], []
     u0_coarse = None
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dns_ms = 0.0
@@ -237,6 +237,7 @@ def make_dataset(fine_n=256, coarse_n=64, nu=1.5e-3, E_target=1.5, spinup=2000, 
         ub = box_filter(u, fine, coarse)
         if u0_coarse is None:
             u0_coarse = ub.clone()
+        U.append(ub)
         X[s] = velocity_gradients(ub, coarse)
         Y[s] = sgs_stress(u, fine, coarse)
         spectra.append(_spectrum(ub, coarse, kc))
@@ -245,7 +246,7 @@ def make_dataset(fine_n=256, coarse_n=64, nu=1.5e-3, E_target=1.5, spinup=2000, 
         A.append(float(b["eps"]) / (2.0 * float(b["E"])))  # hold-energy A = 2 nu Omega / 2E
         if log and s % 20 == 0:
             log(f"snapshot {s}: E={float(b['E']):.4f}")
-    return dict(X=X, Y=Y, spectra=torch.stack(spectra), A=A, E_filtered=E_f, dt=dt, nu=nu,
+    return dict(X=X, Y=Y, U=torch.stack(U), spectra=torch.stack(spectra), A=A, E_filtered=E_f, dt=dt, nu=nu,
                 dns_ms_per_step=dns_ms / (snapshots * every),
                 u0_coarse=u0_coarse, fine=fine, coarse=coarse, wall_s=time.perf_counter() - t0)
 
@@ -395,3 +396,140 @@ def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True
         closure.check_errors()
     return dict(spectrum=spec / max(n, 1), ms_per_step=e0.elapsed_time(e1) / 200, dt=dt, energies=energies,
                 finite=bool(torch.isfinite(u).all()))
+
+
+# ---------------------------------------------------------------------------
+# a-posteriori tuning of the closure through the discrete adjoint
+# ---------------------------------------------------------------------------
+
+def spectrum_log_loss(u_hat, grid, logT):
+    """L = sum_s (log E_s(u) - logT_s)^2 over shells s = 1..len(logT) (E_s the
+    shell energies of `energy_spectrum`) and its cotangent with respect to
+    u_hat (dL/dRe + i dL/dIm of every stored entry):
+    2 (log E_s - logT_s) / E_s * w / N^6 * u_hat on the modes of shell s."""
+    S = logT.numel()
+    k0 = 2 * torch.pi / grid.Lx
+    shp = u_hat.shape[1:]
+    shell = torch.floor(torch.sqrt(grid.k2) / k0 + 0.5).to(torch.int64).expand(shp).reshape(-1)
+    w = grid.weights.to(torch.float64).expand(shp).reshape(-1)
+    n2 = float(grid.Nx * grid.Ny * grid.Nz) ** 2
+    a2 = (u_hat.abs() ** 2).sum(0).reshape(-1).to(torch.float64)
+    E = torch.bincount(shell.clamp(max=S + 1), weights=w * a2, minlength=S + 2)[: S + 1] / (2 * n2)
+    r = torch.log(E[1:]) - logT.to(E.device, torch.float64)
+    coef = torch.zeros(S + 2, dtype=torch.float64, device=u_hat.device)
+    coef[1 : S + 1] = 2 * r / E[1:]
+    c = (coef[shell.clamp(max=S + 1)] * w / n2).reshape(shp)
+    return float((r ** 2).sum()), (c.to(u_hat.real.dtype) * u_hat).contiguous()
+
+
+def les_window_grad(step, u0, nsteps, loss_fn):
+    """Reverse-mode gradient of ``loss_fn(u_n)`` (returning the loss and its
+    cotangent) after ``nsteps`` LES steps of `FusedLESStep` ``step`` (lag off)
+    from u0, with respect to the closure's master parameters and to u0.
+
+    The forward keeps every state (the coarse states are small); the backward
+    runs, step by step from the last, the hand-written transposes:
+    the RK4 step with its held force (``hit_rk4_step_forced_vjp``: the state's
+    and the force's cotangents), the force f = P(-1j k_j rfftn(tau)_ij)
+    (``hit_sgs_force_vjp``), the MLP (``hit_mlp_vjp``: parameter and input
+    cotangents) and the velocity gradients (``hit_velocity_gradients_vjp``),
+    the last two adding the closure's path to the state's cotangent.
+    Returns (loss, parameter cotangents in the order of ``closure.params``,
+    cotangent of u0, final state)."""
+    from .forcing import native_params
+    g = step.grid
+    model = step.closure
+    if model is None or step.lag:
+        raise ValueError("les_window_grad needs a closure and lag=False")
+    states = [_check_state(u0, g)]
+    for _ in range(int(nsteps)):
+        states.append(step(states[-1]))
+    L, lam = loss_fn(states[-1])
+    prm = native_params(step.params.nu, step.params.forcing, 0)
+    if prm is None:
+        raise ValueError("les_window_grad needs a built-in forcing")
+    P = g.Nx * g.Ny * g.Nz
+    st = nat.stream_ptr(g.device)
+    gsum = [torch.zeros_like(q) for q in model.params]
+    tbar = torch.empty(6, P, dtype=g.dtype, device=g.device)
+    fbar = torch.empty_like(lam)
+    for i in range(len(states) - 2, -1, -1):
+        u = states[i]
+        f = step.force(u)  # recomputed; leaves the gradient fields in step._grads
+        ub = torch.empty_like(u)
+        nat.call("hit_rk4_step_forced_vjp", g.plan.handle, nat.ptr(u), prm, nat.ptr(f), float(step.dt), 0.0,
+                 nat.ptr(lam), nat.ptr(ub), nat.ptr(fbar), None, st)
+        nat.call("hit_sgs_force_vjp", g.plan.handle, nat.ptr(fbar), nat.ptr(tbar), st)
+        xbar, gp = model.vjp(step._grads, tbar)
+        nat.call("hit_velocity_gradients_vjp", g.plan.handle, nat.ptr(xbar.to(g.dtype).contiguous()), nat.ptr(ub), st)
+        for acc, d in zip(gsum, gp):
+            acc += d
+        lam = ub
+    model.check_errors()
+    nat.check_device("les_window_grad")
+    return L, gsum, lam, states[-1]
+
+
+def train_a_posteriori(data, model, iters=40, window=64, lr=3e-4, clip=1.0, tau_relax=0.5, seed=0, log=None):
+    """Fine-tune a closure through the LES itself: each iteration runs the LES
+    for ``window`` steps from a filtered DNS snapshot (the hold-energy forcing
+    of `run_les`) and takes an Adam step on the gradient of the squared
+    log-error of the final LES spectrum (shells 1..k_c) against the
+    time-averaged filtered DNS spectrum, from `les_window_grad`; gradients
+    are clipped to global norm ``clip``.  Returns the loss history."""
+    coarse = data["coarse"]
+    kc = coarse.Nx // 3
+    logT = torch.log(data["spectra"].mean(0)[:kc]).to(coarse.device)
+    E_res = sum(data["E_filtered"]) / len(data["E_filtered"])
+    p = NSParams(nu=data["nu"], forcing=HoldEnergyForcing(E_res, data["nu"], tau=tau_relax))
+    U = data["U"]
+    dt = data.get("dt_les") or cfl_dt(U[0], coarse, 0.5)
+    for q in model.params:
+        q.requires_grad_(False)
+    opt = torch.optim.Adam(model.params, lr=lr)
+    gen = torch.Generator().manual_seed(seed)
+    hist = []
+    for it in range(iters):
+        s = int(torch.randint(U.shape[0], (1,), generator=gen))
+        step = FusedLESStep(coarse, model, p, dt)
+        L, grads, _, _ = les_window_grad(step, U[s].clone(), window, lambda u: spectrum_log_loss(u, coarse, logT))
+        norm = float(torch.sqrt(sum((d.double() ** 2).sum() for d in grads)))
+        scale = min(1.0, clip / norm) if norm > 0 else 1.0
+        for q, d in zip(model.params, grads):
+            q.grad = d * scale
+        opt.step()
+        model._packed = None
+        model._physical = None
+        hist.append((it, s, L, norm))
+        if log:
+            log(f"a-posteriori {it}: snapshot {s}, loss {L:.4f}, |grad| {norm:.3g}")
+    return hist
+
+
+def run_spectral_eddy_viscosity_les(data, steps, discard, coef=1.0, sample_every=50, tau_relax=0.5):
+    """The coarse LES with the classical closure that needs no network: the
+    Chollet-Lesieur spectral eddy viscosity
+        nu_t(k) = coef C_K^(-3/2) (0.441 + 15.2 exp(-3.03 k_c / k)) sqrt(E(k_c) / k_c),
+    C_K = 1.4 and E(k_c) the LES's own shell-k_c energy at the start of each
+    step, applied as the force -nu_t(k) k^2 u_hat held over the step, under the
+    hold-energy forcing of `run_les`.  Returns the spectrum of shells 1..k_c
+    averaged over the samples taken every ``sample_every`` steps after
+    ``discard``."""
+    g, nu = data["coarse"], data["nu"]
+    kc = g.Nx // 3
+    E_res = sum(data["E_filtered"]) / len(data["E_filtered"])
+    p = NSParams(nu=nu, forcing=HoldEnergyForcing(E_res, nu, tau=tau_relax))
+    kmag = torch.sqrt(g.k2).clamp_min(1e-6)
+    profile = (coef * 1.4 ** -1.5 * (0.441 + 15.2 * torch.exp(-3.03 * kc / kmag)) * g.k2).to(g.dtype)
+    rhs = make_ns_rhs(g)
+    u = data["u0_coarse"].clone()
+    dt = data.get("dt_les") or cfl_dt(u, g, 0.5)
+    total, count = torch.zeros(kc, dtype=torch.float64), 0
+    for i in range(1, steps + 1):
+        Ekc = max(float(energy_spectrum(u, g)[1][kc - 1]), 0.0)
+        f = (-(Ekc / kc) ** 0.5 * profile) * u
+        u = rk4_step(rhs, u, p, dt, 0.0, f_ext=f)
+        if i % sample_every == 0 and i > discard:
+            total += _spectrum(u, g, kc)
+            count += 1
+    return total / max(count, 1)

@@ -537,79 +537,6 @@ def run_kernel_rooflines(args):
     return 0
 
 
-def spectral_eddy_viscosity_les(data, steps, discard, coef=1.0, sample_every=50):
-    """The coarse LES with a classical spectral closure instead of the MLP:
-    the Chollet-Lesieur eddy viscosity nu_t(k) = coef C_K^(-3/2) (0.441 + 15.2
-    exp(-3.03 k_c / k)) sqrt(E(k_c) / k_c) (C_K = 1.4, E(k_c) the LES's own
-    shell-k_c energy each step), applied as the force -nu_t(k) k^2 u_hat held
-    over each RK4 step, under the same hold-energy forcing as `les.run_les`.
-    Returns the time-averaged spectrum of shells 1..k_c."""
-    h3 = importlib.import_module("3dhit_b200")
-    fmod = importlib.import_module("3dhit_b200.forcing")
-    g, nu = data["coarse"], data["nu"]
-    kc = g.Nx // 3
-    E_res = sum(data["E_filtered"]) / len(data["E_filtered"])
-    p = h3.NSParams(nu=nu, forcing=fmod.HoldEnergyForcing(E_res, nu, tau=0.5))
-    shape = coef * 1.4 ** -1.5 * (0.441 + 15.2 * torch.exp(-3.03 * kc / g.k2.sqrt().clamp_min(1e-6)))
-    rhs = h3.make_ns_rhs(g)
-    u = data["u0_coarse"].clone()
-    dt = h3.cfl_dt(u, g, 0.5)
-    spec, n = torch.zeros(kc, dtype=torch.float64), 0
-    for i in range(1, steps + 1):
-        Ekc = max(float(h3.energy_spectrum(u, g)[1][kc - 1]), 0.0)
-        f = (-(shape * g.k2) * math.sqrt(Ekc / kc)).to(u.dtype) * u
-        u = h3.rk4_step(rhs, u, p, dt, 0.0, f_ext=f)
-        if i % sample_every == 0 and i > discard:
-            spec += torch.as_tensor(h3.energy_spectrum(u, g)[1][:kc], dtype=torch.float64)
-            n += 1
-    return spec / max(n, 1)
-
-
-def closure_diagnosis(les, data, model, args):
-    """Where the LES spectrum error comes from: the drift of the filtered DNS
-    spectrum over its snapshots; the LES over exactly the DNS's sampling window
-    (LES samples at the snapshot times, dt = 1/12 of the snapshot interval);
-    the LES under other forcings (hold-energy with relaxation time 0.05, and a
-    constant Lundgren coefficient equal to the DNS's mean); the closure scaled
-    by 0.7 and 1.4; the classical Chollet-Lesieur spectral eddy viscosity in
-    place of the MLP (coefficient 1 and 0.5)."""
-    fmod = importlib.import_module("3dhit_b200.forcing")
-    S = data["spectra"]
-    q = max(1, S.shape[0] // 5)
-
-    def r4(t):
-        return [round(float(x), 4) for x in t]
-
-    def errs(ratio):
-        return {"max": round(float((ratio - 1).abs().max()), 4), "mean": round(float((ratio - 1).abs().mean()), 4),
-                "ratio_Ek": r4(ratio)}
-
-    out = {"dns_first_fifth": r4(S[:q].mean(0)), "dns_last_fifth": r4(S[-q:].mean(0)),
-           "dns_A_first_last": [data["A"][0], data["A"][-1]]}
-    ref = S.mean(0)
-    m = 12
-    win = dict(data, dt_les=args.cl_every * data["dt"] / m)
-    for name, cl in (("no_closure", None), ("closure", model)):
-        r = les.run_les(win, cl, steps=m * (S.shape[0] - 1), sample_every=m, discard=0)
-        out["same_window_" + name] = errs(r["spectrum"] / S[1:].mean(0))
-    nu, E_res = data["nu"], sum(data["E_filtered"]) / len(data["E_filtered"])
-    A_mean = sum(data["A"]) / len(data["A"])
-    base = model.sgs_scale
-    for name, forcing, sc in (("holdE_tau0.05", fmod.HoldEnergyForcing(E_res, nu, tau=0.05), 1.0),
-                              ("linear_meanA", fmod.LinearForcing(A=A_mean), 1.0),
-                              ("linear_meanA_scale0.7", fmod.LinearForcing(A=A_mean), 0.7),
-                              ("linear_meanA_scale1.4", fmod.LinearForcing(A=A_mean), 1.4)):
-        model.sgs_scale, model._physical = base * sc, None
-        r = les.run_les(data, model, steps=args.cl_les_steps, discard=args.cl_les_steps // 5, forcing=forcing)
-        out["closure_" + name] = dict(errs(r["spectrum"] / ref), energy_first_last=[r["energies"][0],
-                                                                                     r["energies"][-1]])
-    model.sgs_scale, model._physical = base, None
-    for coef in (1.0, 0.5):
-        spec = spectral_eddy_viscosity_les(data, args.cl_les_steps, args.cl_les_steps // 5, coef=coef)
-        out[f"chollet_lesieur_{coef}"] = errs(spec / ref)
-    return out
-
-
 def run_closure(args):
     """Learned SGS closure (Lundgren hold-energy forced DNS on F^3, sharp
     spectral filter to C^3 at k_c = C/3, MLP 9 -> 64x3 -> 6 on the tensor
@@ -632,18 +559,34 @@ def run_closure(args):
     ref = data["spectra"].mean(0)
     kc = data["coarse"].Nx // 3
     out = {}
-    for name, cl, lag in (("no_closure", None, False), ("closure", model, False), ("closure_lagged", model, True)):
+
+    def les_record(name, cl, lag):
         r = les.run_les(data, cl, steps=args.cl_les_steps, discard=args.cl_les_steps // 5, lag=lag)
         rel = (r["spectrum"] / ref - 1).abs()
         T = args.cl_les_steps * r["dt"]
         dns_wall = T / data["dt"] * data["dns_ms_per_step"]
         out[name] = {"max_rel_err_Ek": float(rel.max()), "mean_rel_err_Ek": float(rel.mean()),
                      "ratio_Ek": [round(float(x), 4) for x in r["spectrum"] / ref], "ms_per_step": r["ms_per_step"],
-                     "dt": r["dt"], "finite": r["finite"], "wall_ratio_dns_over_les": dns_wall / (args.cl_les_steps *
-                                                                                                r["ms_per_step"]),
+                     "dt": r["dt"], "finite": r["finite"],
+                     "wall_ratio_dns_over_les": dns_wall / (args.cl_les_steps * r["ms_per_step"]),
                      "energy_first_last": [r["energies"][0], r["energies"][-1]] if r["energies"] else None}
+
+    for name, cl, lag in (("no_closure", None, False), ("closure", model, False), ("closure_lagged", model, True)):
+        les_record(name, cl, lag)
+    # the classical method without a network: Chollet-Lesieur spectral eddy viscosity
+    cl_spec = les.run_spectral_eddy_viscosity_les(data, args.cl_les_steps, args.cl_les_steps // 5)
+    out["chollet_lesieur"] = {"max_rel_err_Ek": float((cl_spec / ref - 1).abs().max()),
+                              "mean_rel_err_Ek": float((cl_spec / ref - 1).abs().mean()),
+                              "ratio_Ek": [round(float(x), 4) for x in cl_spec / ref]}
+    # a-posteriori tuning through the discrete adjoint of the LES
+    t1 = time.perf_counter()
+    apost = les.train_a_posteriori(data, model, iters=args.cl_apost_iters, window=args.cl_apost_window,
+                                   lr=args.cl_apost_lr, log=log)
+    t_apost = time.perf_counter() - t1
+    les_record("closure_a_posteriori", model, False)
+    les_record("closure_a_posteriori_lagged", model, True)
     line = {"metric": f"closure-LES {args.cl_coarse}^3 vs filtered {args.cl_fine}^3 DNS: max E(k) rel err, k<=k_c",
-            "value": out["closure"]["max_rel_err_Ek"], "unit": "fraction", "higher_is_better": False,
+            "value": out["closure_a_posteriori"]["max_rel_err_Ek"], "unit": "fraction", "higher_is_better": False,
             "fallback_value": out["no_closure"]["max_rel_err_Ek"],
             "config": {"workload": f"Lundgren hold-E DNS {args.cl_fine}^3 (nu=1.5e-3, E_t=1.5, CFL 0.5), "
                                    f"{args.cl_spinup} spin-up steps, {args.cl_snapshots} snapshots every "
@@ -652,10 +595,11 @@ def run_closure(args):
                                    f"(relaxation 0.5); SGS stress once per RK4 step; closure rescaled to the DNS SGS "
                                    f"energy transfer"},
             "dns_ms_per_step": data["dns_ms_per_step"], "dns_dt": data["dt"], "mean_A": sum(data["A"]) / len(data["A"]),
-            "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train},
-            "no_closure": out["no_closure"], "closure": out["closure"], "closure_lagged": out["closure_lagged"]}
-    if args.cl_diagnose:
-        line["diagnosis"] = closure_diagnosis(les, data, model, args)
+            "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train, "a_posteriori": t_apost},
+            "a_posteriori": {"iters": args.cl_apost_iters, "window": args.cl_apost_window, "lr": args.cl_apost_lr,
+                             "loss_first_last_10": [sum(h[2] for h in apost[:10]) / max(1, len(apost[:10])),
+                                                    sum(h[2] for h in apost[-10:]) / max(1, len(apost[-10:]))]},
+            **out}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -698,8 +642,9 @@ def main():
     ap.add_argument("--cl-every", type=int, default=50)
     ap.add_argument("--cl-train-steps", type=int, default=400)
     ap.add_argument("--cl-les-steps", type=int, default=5000)
-    ap.add_argument("--cl-diagnose", action="store_true",
-                    help="closure run: add the spectrum-error diagnosis (DNS drift, same-window LES, other forcings)")
+    ap.add_argument("--cl-apost-iters", type=int, default=60)
+    ap.add_argument("--cl-apost-window", type=int, default=64)
+    ap.add_argument("--cl-apost-lr", type=float, default=3e-4)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

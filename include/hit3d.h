@@ -273,6 +273,42 @@ int hit_mlp_train_grads(const hit_mlp_weights *w, const float *x,
                         float *dW1, float *dW2, float *dW3, float *dW4,
                         double *loss_dev, int *err_dev, void *stream);
 
+/* Discrete adjoint of the coarse LES step with the learned closure (no
+ * reference counterpart: the reference has no LES; its AD model is jax.vjp
+ * through rollout, src/hit3d/integrators.py:5-9,41-53).  Cotangents follow
+ * hit_rhs_vjp (dL/dRe + i dL/dIm of every stored entry).
+ *
+ * hit_rk4_step_forced_vjp: transpose of hit_rollout_forced(..., nsteps = 1),
+ * the RK4 step with the force f_ext held over its stages: u_bar = (d step /
+ * d u)^T ct, f_bar (nullable) = (d step / d f_ext)^T ct = P (sum of the
+ * stages' cotangents), P the dealias mask and projection; param_ct as in
+ * hit_rk4_step_vjp.  The stage inputs are recomputed on the general path. */
+int hit_rk4_step_forced_vjp(hit_plan *plan, const void *u_hat,
+                            const hit_params *params, const void *f_ext,
+                            double dt, double t, const void *ct, void *u_bar,
+                            void *f_bar, double *param_ct, void *stream);
+/* tau_bar (DEVICE, 6 x Nx*Ny*Nz physical, the plan's dtype): the cotangent of
+ * the physical stress tau whose force hit_sgs_force(rfftn(tau)) has cotangent
+ * f_bar (reference layout). */
+int hit_sgs_force_vjp(hit_plan *plan, const void *f_bar, void *tau_bar,
+                      void *stream);
+/* u_bar (reference layout) += the cotangent of u_hat whose velocity gradients
+ * (hit_velocity_gradients) have cotangent grads_bar (9 x Nx*Ny*Nz physical). */
+int hit_velocity_gradients_vjp(hit_plan *plan, const void *grads_bar,
+                               void *u_bar, void *stream);
+/* Vector-Jacobian product of the closure MLP at inputs x (feature f of point
+ * p at x[f*x_sf + p*x_sp]) for the output cotangent ybar (component c at
+ * ybar[c*y_sf + p*y_sp]): the parameter cotangents dW1..dW4 in the layout of
+ * hit_mlp_train_grads, and, when xbar is not NULL, the input cotangent (same
+ * layout as x); w1 is W1 as a bf16 [16][64] array (rows 0-8 used, the rest
+ * zero), needed only for xbar.  P a multiple of 16; workspace of
+ * hit_mlp_workspace_bytes(P) bytes. */
+int hit_mlp_vjp(const hit_mlp_weights *w, const void *w1, const float *x,
+                int64_t x_sf, int64_t x_sp, const float *ybar, int64_t y_sf,
+                int64_t y_sp, int64_t P, void *workspace, float *dW1,
+                float *dW2, float *dW3, float *dW4, float *xbar, int *err_dev,
+                void *stream);
+
 /* energy_spectrum without any device allocation.  No counterpart in the
  * reference: it serves callers that cannot allocate device memory -- code
  * running while its stream is being captured into a CUDA graph, an XLA custom
