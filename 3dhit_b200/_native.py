@@ -77,6 +77,7 @@ SIGNATURES = {
     "hit_set_wait_limit": (_i, [_i]),
     "hit_rk4_step_forced_vjp": (_i, [_vp, _vp, _PP, _vp, _d, _d, _vp, _vp, _vp, _vp, _vp]),
     "hit_sgs_force_vjp": (_i, [_vp, _vp, _vp, _vp]),
+    "hit_axis_fft": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp]),
     "hit_velocity_gradients_vjp": (_i, [_vp, _vp, _vp, _vp]),
     "hit_mlp_vjp": (_i, [_vp, _vp, _vp, _i64, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hit_rollout_forced": (_i, [_vp, _vp, _PP, _vp, _d, _i64, _d, _vp, _vp]),

@@ -617,6 +617,56 @@ template <typename T> int to_spectral_impl(hit_plan* p, const void* u, int nc, v
   return HIT_OK;
 }
 
+// One axis of the 3-D transform on reference-layout arrays (ncomp, Nx, Ny,
+// Nzh), unnormalised: axis 0 / 1 complex along x / y (in and out distinct,
+// same layout); axis 2 the real transform along z between (ncomp, Nx, Ny, Nzh)
+// complex and (ncomp, Nx, Ny, Nz) real (c2r when inverse: the imaginary parts
+// of the kz = 0 and Nyquist entries are dropped), through the padded workspace.
+template <typename T>
+int axis_fft_impl(hit_plan* p, const void* in, void* out, int nc, int axis, int inverse, cudaStream_t st) {
+  const Geom g = make_geom(p->Nx, p->Ny, p->Nz, false);
+  const bool inv = inverse != 0;
+  if (axis == 0 || axis == 1) {
+    const int N = axis == 0 ? g.Nx : g.Ny;
+    const int W = axis_tile_w<T>(N);
+    AxisArgs<T> a{};
+    a.src = static_cast<const V2<T>*>(in);
+    a.dst = static_cast<V2<T>*>(out);
+    a.s_c = a.d_c = (long long)g.Nx * g.Ny * g.Nzh;
+    a.s_a = a.d_a = axis == 0 ? (long long)g.Ny * g.Nzh : g.Nzh;
+    a.s_o = a.d_o = axis == 0 ? g.Nzh : (long long)g.Ny * g.Nzh;
+    a.Min = a.Mout = N;
+    a.hin = a.hout = N / 2;
+    a.nz = g.Nzh;
+    a.tw = tw_of<T>(p);
+    HIT_CK(launch_axis<T>(N, inv, a, (g.Nzh + W - 1) / W, axis == 0 ? g.Ny : g.Nx, nc, st));
+    return HIT_OK;
+  }
+  int rc;
+  if ((rc = ensure(p->xws, (size_t)nc * g.Nx * g.Ny * g.Mzp * sizeof(V2<T>)))) return rc;
+  const size_t es = sizeof(V2<T>);
+  const size_t rows = (size_t)nc * g.Nx * g.Ny;
+  ZRealArgs<T> z{};
+  z.cbuf = vp<T>(p->xws);
+  z.cc_stride = (long long)g.Nx * g.Ny * g.Mzp;
+  z.rc_stride = (long long)g.Nx * g.Ny * g.Nz;
+  z.nrows = g.Nx * g.Ny;
+  z.Mz = g.Nzh;
+  z.Mzp = g.Mzp;
+  z.scale = T(1);
+  z.tw = tw_of<T>(p);
+  if (inv) {
+    HIT_CK(cudaMemcpy2DAsync(p->xws.p, g.Mzp * es, in, g.Nzh * es, g.Nzh * es, rows, cudaMemcpyDeviceToDevice, st));
+    z.rbuf = static_cast<T*>(out);
+    HIT_CK(launch_zc2r<T>(g.H, z, nc, st));
+  } else {
+    z.rbuf = const_cast<T*>(static_cast<const T*>(in));
+    HIT_CK(launch_zr2c<T>(g.H, z, nc, st));
+    HIT_CK(cudaMemcpy2DAsync(out, g.Nzh * es, p->xws.p, g.Mzp * es, g.Nzh * es, rows, cudaMemcpyDeviceToDevice, st));
+  }
+  return HIT_OK;
+}
+
 // spectrum / budget over the reference layout
 template <typename T>
 int diag_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double* E, double* Ec, double* budget,
@@ -1179,6 +1229,14 @@ int hit_rk4_step_forced_vjp(hit_plan* p, const void* u_hat, const hit_params* pr
     return fail(HIT_E_UNSUPPORTED, "the integrating-factor RK4 step has no transpose");
   DeviceGuard dg(p->device);
   return DISPATCH(p, forced_vjp_entry)(p, u_hat, pr, f_ext, dt, ct, u_bar, f_bar, param_ct, (cudaStream_t)stream);
+}
+
+int hit_axis_fft(hit_plan* p, const void* in, void* out, int ncomp, int axis, int inverse, void* stream) {
+  if (!p || !in || !out) return fail(HIT_E_INVALID, "NULL argument");
+  if (ncomp < 1 || axis < 0 || axis > 2) return fail(HIT_E_INVALID, "axis_fft: ncomp >= 1, axis in {0, 1, 2}");
+  if (axis < 2 && in == out) return fail(HIT_E_INVALID, "axis_fft: in and out must differ");
+  DeviceGuard dg(p->device);
+  return DISPATCH(p, axis_fft_impl)(p, in, out, ncomp, axis, inverse, (cudaStream_t)stream);
 }
 
 int hit_sgs_force_vjp(hit_plan* p, const void* f_bar, void* tau_bar, void* stream) {

@@ -273,6 +273,18 @@ int hit_mlp_train_grads(const hit_mlp_weights *w, const float *x,
                         float *dW1, float *dW2, float *dW3, float *dW4,
                         double *loss_dev, int *err_dev, void *stream);
 
+/* One axis of the 3-D transform, unnormalised, on reference-layout arrays of
+ * the plan's grid: axis 0 / 1 the complex transform along x / y of
+ * (ncomp, Nx, Ny, Nz/2+1) complex arrays (in != out); axis 2 the real
+ * transform along z between (ncomp, Nx, Ny, Nz/2+1) complex and
+ * (ncomp, Nx, Ny, Nz) real (inverse = c2r, dropping the imaginary parts of
+ * the kz = 0 and Nyquist entries as irfftn does; else r2c).  inverse != 0
+ * selects exp(+2 pi i nk/N).  The building block of the slab-decomposed RHS
+ * (3dhit_b200/slab.py): to_physical = z c2r after the x and y inverses
+ * (src/hit3d/grid.py:181-183), each rank transforming its slab. */
+int hit_axis_fft(hit_plan *plan, const void *in, void *out, int ncomp,
+                 int axis, int inverse, void *stream);
+
 /* Discrete adjoint of the coarse LES step with the learned closure (no
  * reference counterpart: the reference has no LES; its AD model is jax.vjp
  * through rollout, src/hit3d/integrators.py:5-9,41-53).  Cotangents follow
