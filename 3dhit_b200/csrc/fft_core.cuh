@@ -204,7 +204,8 @@ __device__ __forceinline__ void fft_stage_io(V2<T>* __restrict__ A, V2<T>* __res
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if constexpr (SRC == 0) {
-          if constexpr (std::is_invocable<LD&, int, int, int>::value) v[r] = ld(b + r * NB, col, r);
+          if constexpr (std::is_invocable<LD&, int, int, int, int>::value) v[r] = ld(b + r * NB, col, r, c);
+          else if constexpr (std::is_invocable<LD&, int, int, int>::value) v[r] = ld(b + r * NB, col, r);
           else v[r] = ld(b + r * NB, col);
         } else if constexpr (NB % 8 == 0) {
           v[r] = src[ADDR::at(b, col) + ADDR::step(r * NB)];
@@ -261,8 +262,8 @@ __device__ __forceinline__ void fft_stages_io(V2<T>* A, V2<T>* B, const V2<T>* t
 // thread's butterflies are t = threadIdx.x + c*NT (col = t % NCOLS, b = t /
 // NCOLS); ld may take a third argument r and st a fourth, the index of the
 // value within the butterfly (position b + r*N/R in the first stage, j + r*P
-// in the last), and st a fifth, the thread's butterfly index c, so a caller
-// can keep a thread's inputs or outputs in registers.  The caller synchronises before ld reads shared memory written by
+// in the last), and ld a fourth and st a fifth, the thread's butterfly index
+// c, so a caller can keep a thread's inputs or outputs in registers.  The caller synchronises before ld reads shared memory written by
 // other threads and after st writes shared memory that other threads read.
 // after_stage0() (optional) runs once every thread has finished the first
 // stage, when the loader's source may be reused.

@@ -15,11 +15,13 @@
 //         projection (grid.py:166-178), viscous term (navierstokes.py:95) and
 //         the RK4 stage algebra (integrators.py:32-38), then -- fused -- the
 //         next stage's k_p1 on the tile it just produced.
+#include <algorithm>
 #include <cstdint>
 #include <type_traits>
 
 #include "fft_core.cuh"
 #include "kernels.h"
+#include "tc_common.cuh"
 #include "tma.cuh"
 
 namespace hit {
@@ -661,6 +663,274 @@ __global__ void __launch_bounds__(NTH) k_p3(P3Args<T> a, int nzt, int ntiles) {
 }
 
 // ---------------------------------------------------------------------------
+// k_p3m: P3 for float32 columns of 512 points, two 256-thread CTAs per SM,
+// with the tile's spectral values parked in tensor memory (TMEM).
+//
+// The register-mode k_p3 keeps the three nonlinear-term components of a
+// thread's positions in registers from the x-forward through the epilogue to
+// the fused x-inverse.  That needs one butterfly per thread (512 threads per
+// 8-column tile), and with its staging ring one CTA fills an SM, so every
+// stage barrier idles the whole SM.  Here a thread owns two butterflies per
+// stage (256 threads per tile) and parks what it would hold -- 3 components x
+// 16 positions, then the outputs of one inverse transform that the curl needs
+// later -- in its own TMEM lane: 128 32-bit columns per thread, 256 per CTA,
+// so two CTAs take the SM's 512 columns and one CTA's barriers overlap the
+// other's work.  The epilogue's state rows are staged pass by pass into the
+// two FFT buffers, which are idle between the forward and inverse transforms.
+//
+// TMEM columns of a thread (from its base): component c of position
+// b_i + r N/8 (butterfly i = 0, 1, b_i = threadIdx.x / W + i * 256 / W) at
+// 32 c + 16 i + 2 r (re, im); columns 96 + 16 i + 2 r hold the kept outputs of
+// an inverse transform.  Warps w and w + 4 share TMEM lanes 32 (w % 4) .. +31
+// and take columns [0, 128) and [128, 256) of the CTA's allocation.
+// ---------------------------------------------------------------------------
+constexpr int P3M_THREADS = 256;
+constexpr int P3M_COLS = 256;  // TMEM columns per CTA
+
+template <int N, int W> __host__ __device__ constexpr bool p3m_fits() {
+  return fft_radix(N, 0) == 8 && fft_radix(N, fft_nstages(N) - 1) == 8 && (N / 8) * W == 2 * P3M_THREADS &&
+         p3_ring_slot<N, W>() <= skew8_slots(N, W);
+}
+
+// x-inverse of the new stage input (in TMEM) and of w = i k x u, as p1_body.
+template <int N, int W>
+__device__ __forceinline__ void p1m_body(float2* A, float2* B, int j, int z0, const Geom& g, const KTab<float>& kt,
+                                         const float2* tws, float2* t6, long long t_c, long long t_x, uint32_t tm) {
+  constexpr int NTH = P3M_THREADS;
+  const int fy = full_pos(j, g.hy, g.My, g.Ny);
+  const float ky = kt.ky[fy];
+  float2* out = t6 + (long long)j * g.Mzp + z0;
+  const int z = z0 + threadIdx.x % W;  // NTH is a multiple of W: the column of both butterflies
+  const float kz = z < g.Nzh ? kt.kz[z] : 0.f;
+  auto put = [&](int q, int pos, int col, float2 v) { out[q * t_c + (long long)pos * t_x + col] = v; };
+  float lb[16], kb[8], ob[16];
+  // first-stage loader of component c (times kx when kxs): the 8 values of
+  // butterfly i come from TMEM in one load
+  auto src = [&](int c, bool kxs) {
+    return [&, c, kxs](int pos, int, int r, int i) {
+      if (r == 0) tc::tmem_ld16(tm + 32 * c + 16 * i, lb);
+      const float2 v = make_float2(lb[2 * r], lb[2 * r + 1]);
+      return kxs ? cscale(v, kt.kx[pos]) : v;
+    };
+  };
+  auto kept = [&](int r, int i) {  // in two halves: fewer live registers in the last stage
+    if (r % 4 == 0) tc::tmem_ld8(tm + 96 + 16 * i + 2 * r, kb);
+    return make_float2(kb[2 * (r % 4)], kb[2 * (r % 4) + 1]);
+  };
+  auto keep = [&](float2 v, int r, int i) {
+    ob[2 * r] = v.x;
+    ob[2 * r + 1] = v.y;
+    if (r == 7) tc::tmem_st16(tm + 96 + 16 * i, ob);
+  };
+  // u_x (kept)
+  fft_io<float, N, W, NTH, TileAddr<N, W>, true>(A, B, tws, src(0, false), [&](int pos, int col, float2 v, int r, int i) {
+    put(0, pos, col, v);
+    keep(v, r, i);
+  });
+  tc::tmem_wait_st();
+  // kx u_y -> w_z = i (X_y - ky u_x)
+  fft_io<float, N, W, NTH, TileAddr<N, W>, true>(A, B, tws, src(1, true), [&](int pos, int col, float2 v, int r, int i) {
+    put(5, pos, col, cmul_i(csub(v, cscale(kept(r, i), ky))));
+  });
+  // kx u_z -> w_y = i (kz u_x - X_z)
+  fft_io<float, N, W, NTH, TileAddr<N, W>, true>(A, B, tws, src(2, true), [&](int pos, int col, float2 v, int r, int i) {
+    put(4, pos, col, cmul_i(csub(cscale(kept(r, i), kz), v)));
+  });
+  // u_y (kept)
+  fft_io<float, N, W, NTH, TileAddr<N, W>, true>(A, B, tws, src(1, false), [&](int pos, int col, float2 v, int r, int i) {
+    put(1, pos, col, v);
+    keep(v, r, i);
+  });
+  tc::tmem_wait_st();
+  // u_z -> w_x = i (ky u_z - kz u_y)
+  fft_io<float, N, W, NTH, TileAddr<N, W>, true>(A, B, tws, src(2, false), [&](int pos, int col, float2 v, int r, int i) {
+    put(2, pos, col, v);
+    put(3, pos, col, cmul_i(csub(cscale(v, ky), cscale(kept(r, i), kz))));
+  });
+}
+
+// One (ky row, z tile) of k_p3m.  stg holds the staged first nl component.
+template <int N, int W>
+__device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, float2* B, const float2* tws,
+                                         double* red, int j, int z0, int tile, float2* stg, int nzt, int ntiles,
+                                         uint32_t tm) {
+  constexpr int NTH = P3M_THREADS, NB = N / 8;
+  const Geom& g = a.g;
+  constexpr int CPR = W / 2;  // 16-byte chunks per row
+  auto prefetch = [&](int t, int c) {
+    const int jj = t / nzt, zz = (t % nzt) * W;
+    const float2* src = a.t3 + c * a.t_c + (long long)jj * g.Mzp + zz;
+    for (int e = threadIdx.x; e < N * CPR; e += NTH) {
+      const int row = e / CPR, ch = e % CPR;
+      cp_async16(stg + row * W + ch * 2, src + (long long)row * a.t_x + ch * 2);
+    }
+    cp_async_commit();
+  };
+  const long long cbase = (long long)j * g.Mzp + z0;
+  const int nq = a.stage <= 1 ? 3 : 9;  // (array, component): u | s, acc, u
+  // the state rows the epilogue reads, into L2 while the forward transforms run
+  for (int q = 0; q < nq; ++q) {
+    const float2* arr = q < 3 ? (a.stage <= 1 ? a.u : a.s) : (q < 6 ? a.acc : a.u);
+    const float2* base = arr + (q % 3) * a.c_c + cbase;
+    for (int i = threadIdx.x; i < g.Mx; i += NTH) prefetch_l2(base + (long long)i * a.c_x, W * sizeof(float2));
+  }
+  // x-forward of the three nl components; each thread's last-stage outputs go to TMEM
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    cp_async_wait_all();
+    __syncthreads();
+    float ob[16];
+    fft_io<float, N, W, NTH, TileAddr<N, W>, false>(
+        A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; },
+        [&](int, int, float2 v, int r, int i) {
+          ob[2 * r] = v.x;
+          ob[2 * r + 1] = v.y;
+          if (r == 7) tc::tmem_st16(tm + 32 * c + 16 * i, ob);
+        },
+        [&]() {
+          if (c < 2) prefetch(tile, c + 1);
+          else if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, 0);
+        });
+  }
+  tc::tmem_wait_st();
+
+  // epilogue: pass r covers positions r N/8 .. r N/8 + N/8 - 1 (b_i + r N/8 of
+  // every thread); passes whose positions are all outside the stored rows are
+  // skipped.  The state rows of a pass are staged into A or B (a 2-slot ring)
+  // with cp.async, the next pass's while this one is computed.
+  const float2* __restrict__ us_arr = a.stage <= 1 ? a.u : a.s;
+  auto stored = [&](int r) {  // does pass r hold a stored row (uniform)
+    return r * NB < g.hx || (r + 1) * NB > g.hx + (N - g.Mx);
+  };
+  auto next_pass = [&](int r) {  // first pass >= r with stored rows (8: none)
+    while (r < 8 && !stored(r)) ++r;
+    return r;
+  };
+  auto stage_pass = [&](int r, float2* slot) {
+    if (r < 8) {
+      for (int e = threadIdx.x; e < nq * NB * CPR; e += NTH) {
+        const int q = e / (NB * CPR), rem = e % (NB * CPR), lr = rem / CPR, ch = rem % CPR;
+        const int i = compact_row(r * NB + lr, g.hx, g.Mx, N);
+        if (i >= 0) {
+          const float2* arr = q < 3 ? us_arr : (q < 6 ? a.acc : a.u);
+          cp_async16(slot + (q * NB + lr) * W + ch * 2, arr + (q % 3) * a.c_c + cbase + (long long)i * a.c_x + ch * 2);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  const int fy = full_pos(j, g.hy, g.My, g.Ny);
+  const float ky = a.k.ky[fy];
+  const float cf = (a.forcing == 2 || a.forcing == 3) ? (float)a.coef[0] : 0.f;
+  double sE = 0.0, sO = 0.0, sB = 0.0;
+  const int col = threadIdx.x % W, b0 = threadIdx.x / W;
+  const int z = z0 + col;
+  const bool zok = z < g.Mz;
+  const float kz = zok ? __ldg(a.k.kz + z) : 0.f;
+  __syncthreads();  // every thread has left the last forward stage: A and B are free
+  int rc = next_pass(0);
+  int rn = next_pass(rc + 1);
+  stage_pass(rc, A);
+  stage_pass(rn, B);
+  const float zeros[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  int k = 0;
+#pragma unroll 1
+  for (int r = 0; r < 8; ++r) {
+    if (r != rc) {  // no stored rows: the new stage input is zero here
+      tc::tmem_st2x3(tm + 2 * r, 32, zeros);
+      tc::tmem_st2x3(tm + 16 + 2 * r, 32, zeros);
+      continue;
+    }
+    float2* slot = (k & 1) ? B : A;
+    cp_async_wait_group<1>();
+    __syncthreads();
+    float d[12];
+    tc::tmem_ld2x3x2(tm + 2 * r, 32, 16, d);  // [6 i + 2 c]: component c of butterfly i
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int lb = b0 + i * (NTH / W);
+      const int pos = lb + r * NB;
+      const int row = compact_row(pos, g.hx, g.Mx, N);
+      float2 ns[3] = {czero<float>(), czero<float>(), czero<float>()};
+      if (zok && row >= 0) {
+        const float2* sl = slot + lb * W + col;
+        float2 us[3], ac[3], uu[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          us[c] = sl[c * NB * W];
+          if (a.stage >= 2) {
+            ac[c] = sl[(3 + c) * NB * W];
+            uu[c] = sl[(6 + c) * NB * W];
+          }
+        }
+        float2 du[3] = {make_float2(d[6 * i], d[6 * i + 1]), make_float2(d[6 * i + 2], d[6 * i + 3]),
+                        make_float2(d[6 * i + 4], d[6 * i + 5])};
+        const long long o = cbase + (long long)row * a.c_x + col;
+        p3_point(a, pos, fy, z, ky, kz, cf, o, du, us, ac, uu, ns, sE, sO, sB);
+      }
+      const float nv[6] = {ns[0].x, ns[0].y, ns[1].x, ns[1].y, ns[2].x, ns[2].y};
+      tc::tmem_st2x3(tm + 16 * i + 2 * r, 32, nv);
+    }
+    __syncthreads();  // the slot is read: it takes the pass after next
+    const int r2 = next_pass(rn + 1);
+    stage_pass(r2, slot);
+    rc = rn;
+    rn = r2;
+    ++k;
+  }
+  tc::tmem_wait_st();
+  if (a.partial) {
+    block_sum3_f64(sE, sO, sB, red);
+    if (threadIdx.x == 0) {
+      a.partial[3 * tile + 0] = sE;
+      a.partial[3 * tile + 1] = sO;
+      a.partial[3 * tile + 2] = sB;
+    }
+  }
+  if (a.fuse_p1) p1m_body<N, W>(A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x, tm);
+}
+
+template <int N, int W>
+__global__ void __launch_bounds__(P3M_THREADS, 2) k_p3m(P3Args<float> a, int nzt, int ntiles) {
+  static_assert(p3m_fits<N, W>(), "two radix-8 butterflies per thread at the first and last stage");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[96];
+  __shared__ uint32_t tslot;
+  float2* A = reinterpret_cast<float2*>(smem_raw);
+  float2* B = A + skew8_slots(N, W);
+  float2* stg = B + skew8_slots(N, W);  // staged N x W column of the next nl component
+  float2* tws = stg + N * W;
+  fill_stage_twiddles<float, N, false, P3M_THREADS>(tws, a.tw);
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tslot), P3M_COLS);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tm = tslot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(warp >> 2) * 128;
+  pdl_wait();
+  pdl_trigger();
+  if (blockIdx.x < ntiles) {
+    const int jj = blockIdx.x / nzt, zz = (blockIdx.x % nzt) * W;
+    const float2* src = a.t3 + (long long)jj * a.g.Mzp + zz;
+    constexpr int CPR = W / 2;
+    for (int e = threadIdx.x; e < N * CPR; e += P3M_THREADS) {
+      const int row = e / CPR, ch = e % CPR;
+      cp_async16(stg + row * W + ch * 2, src + (long long)row * a.t_x + ch * 2);
+    }
+    cp_async_commit();
+  }
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int j = tile / nzt, z0 = (tile % nzt) * W;
+    p3m_tile<N, W>(a, A, B, tws, red, j, z0, tile, stg, nzt, ntiles, tm);
+  }
+  cp_async_wait_all();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tslot, P3M_COLS);
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 
@@ -850,6 +1120,39 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Ar
                     NTH, smem, st, a, nzt, ntiles);
 }
 
+// k_p3m shared memory: A, B, the staged nl column (N x W) and the twiddles.
+template <int N, int W> constexpr size_t p3m_smem() {
+  return sizeof(float2) * ((size_t)2 * skew8_slots(N, W) + N * W + tw_slots_even<N>());
+}
+
+template <int NN, int W> cudaError_t launch_p3m_v(const P3Args<float>& a, cudaStream_t st) {
+  static PerDevice cache, ready;
+  cudaError_t e = once_per_device(ready, [] { return max_smem(k_p3m<NN, W>, (int)p3m_smem<NN, W>()); });
+  if (e != cudaSuccess) return e;
+  const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
+  // Resident CTAs: the occupancy query counts one CTA per SM for kernels that
+  // allocate tensor memory, so the wave is sized from the SM's shared memory
+  // and registers, at most 2 per SM (two 256-column TMEM allocations fill it).
+  std::atomic<int>* slot = cache.here();
+  int wave = slot ? slot->load(std::memory_order_relaxed) : 0;
+  if (wave == 0) {
+    int dev = 0, sms = 0, smem_sm = 0, regs_sm = 0;
+    cudaFuncAttributes fa{};
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+      return e;
+    if ((e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, k_p3m<NN, W>)) != cudaSuccess) return e;
+    const int by_smem = smem_sm / (int)(p3m_smem<NN, W>() + fa.sharedSizeBytes + 1024);
+    const int by_regs = regs_sm / (P3M_THREADS * ((std::max(fa.numRegs, 1) + 7) / 8 * 8));
+    wave = std::max(1, std::min(std::min(by_smem, by_regs), 512 / P3M_COLS)) * std::max(sms, 1);
+    if (slot) slot->store(wave, std::memory_order_relaxed);
+  }
+  return launch_pdl(k_p3m<NN, W>, ntiles < wave ? std::max(ntiles, 1) : wave, P3M_THREADS, p3m_smem<NN, W>(), st, a,
+                    nzt, ntiles);
+}
+
 // Threads per k_p1/k_p3 CTA: 512 (one CTA per SM at 512- and 1024-point
 // columns); 256 for columns of at most 128 points, whose tiles have at most
 // 128 butterflies per stage, so that the CTA leaves half an SM's registers to
@@ -866,7 +1169,11 @@ template <typename T> cudaError_t launch_p1(const P1Args<T>& a, cudaStream_t st)
 template <typename T> cudaError_t launch_p3(const P3Args<T>& a, cudaStream_t st) {
   return dispatch_len(a.g.Nx, [&](auto nn) {
     constexpr int NN = decltype(nn)::value;
-    return launch_p3_v<T, NN, tile_wp<T>(NN), p_threads<NN>()>(a, st);
+    if constexpr (std::is_same<T, float>::value && NN == 512) {
+      return launch_p3m_v<NN, tile_wp<float>(NN)>(a, st);
+    } else {
+      return launch_p3_v<T, NN, tile_wp<T>(NN), p_threads<NN>()>(a, st);
+    }
   });
 }
 

@@ -104,5 +104,62 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 8 consecutive columns, as tmem_ld16.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 16 consecutive 32-bit columns of this thread's TMEM lane from registers
+// (asynchronous: tmem_wait_st before the columns are read back).
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+      "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+      "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+      "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+      "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+// Two consecutive columns (one complex value) at each of taddr + k*d, k = 0..2.
+__device__ __forceinline__ void tmem_st2x3(uint32_t taddr, uint32_t d, const float (&v)[6]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%3,%4};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x2.b32 [%1], {%5,%6};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x2.b32 [%2], {%7,%8};" ::"r"(taddr),
+      "r"(taddr + d), "r"(taddr + 2 * d), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])),
+      "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5]))
+      : "memory");
+}
+// The loads of tmem_st2x3's pattern at two bases (taddr, taddr + e), with
+// their completion wait in the same asm statement.
+__device__ __forceinline__ void tmem_ld2x3x2(uint32_t taddr, uint32_t d, uint32_t e, float (&v)[12]) {
+  uint32_t r[12];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%12];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%2,%3}, [%13];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%4,%5}, [%14];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%6,%7}, [%15];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%8,%9}, [%16];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%10,%11}, [%17];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11])
+      : "r"(taddr), "r"(taddr + d), "r"(taddr + 2 * d), "r"(taddr + e), "r"(taddr + e + d), "r"(taddr + e + 2 * d)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 12; ++i) v[i] = __uint_as_float(r[i]);
+}
+// Wait until this thread's earlier tcgen05.st have completed.
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 }  // namespace tc
 }  // namespace hit
