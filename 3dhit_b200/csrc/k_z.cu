@@ -241,6 +241,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
   auto below = [](int k, int lo, int hi, int bound) { return hi < bound ? true : (lo >= bound ? false : k < bound); };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = lane / Z::LPR, b = lane % Z::LPR;
+  const ZwMid<H> mid(b);
   const int stg_slots = 6 * Z::ROWS * Mzp;
   float2* stg = tws + Z::TWS + warp * (stg_slots + Z::ROWS * Z::XS);  // [field][row][Mzp]
   float2* xch = stg + stg_slots + q * Z::XS;
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
         w.y = -w.y;
         v[r] = cadd(sm, cmul_i(cmul(w, df)));
       }
-      zw_transform<H, true>(v, xch, tws, b);
+      zw_transform<H, true>(v, xch, tws, b, mid);
       if (c == 5 && grp + nwarps < ngroups) prefetch(grp + nwarps);  // every lane is past its staged reads
       // u x w (navierstokes.py:82-86) in the packed form of the real rows:
       // n0 = u1 w2 - u2 w1, n1 = u2 w0 - u0 w2, n2 = u0 w1 - u1 w0
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
       float2 v[8];
 #pragma unroll
       for (int r = 0; r < 8; ++r) v[r] = c == 0 ? n0[r] : (c == 1 ? n1[r] : n2[r]);
-      zw_transform<H, false>(v, xch, tws, b);
+      zw_transform<H, false>(v, xch, tws, b, mid);
       float2* out = a.buf + c * a.c_stride + (grp * Z::ROWS + q) * Mzp;
       const int partner = q * Z::LPR + ((Z::LPR - b) & (Z::LPR - 1));
 #pragma unroll

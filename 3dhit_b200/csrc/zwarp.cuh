@@ -70,12 +70,47 @@ template <int H, int NTH> __device__ __forceinline__ void zw_fill_twiddles(float
   }
 }
 
+// Middle-stage butterflies of a lane (H = 128, 256: C1 = 8 / R1 per lane).
+// With the plain assignment b1 = b + LPR i, the stores j + 8 r (j = 32
+// (b1 / 8) + b1 % 8) of a half warp at H = 256 put two lanes on 6 of the 8
+// bank pairs they use.  The table below assigns the 64 butterflies of H = 256
+// to (lane, i) so that every middle-stage load (b1 + 64 r) and store of a half
+// warp hits 16 distinct bank pairs under zw_slot: each half warp's 16
+// butterflies are one perfect matching of the bipartite graph joining a
+// butterfly's load bank pair to its store bank pair (4-regular, so four
+// matchings cover it).  Entry [32 i + lane].
+__device__ const unsigned char kZwMid256[64] = {
+    0, 1,  2,  3,  4,  5,  6,  13, 14, 15, 37, 38, 39, 40, 41, 42, 8,  9,  10, 17, 18, 19,
+    20, 21, 28, 29, 30, 31, 47, 52, 56, 57, 7,  11, 12, 16, 32, 33, 34, 35, 36, 43, 44, 45,
+    46, 53, 54, 55, 22, 23, 24, 25, 26, 27, 48, 49, 50, 51, 58, 59, 60, 61, 62, 63};
+
+template <int H> struct ZwMid {
+  static constexpr int R1 = ZW<H>::R1, C1 = R1 > 1 ? 8 / R1 : 1;
+  int k[C1];   // twiddle index b1 % 8
+  int ld[C1];  // exchange slot of input b1 (input r at ld + zw_slot(r H / R1))
+  int st[C1];  // exchange slot of output j (output r at st + zw_slot(8 r))
+  // once per thread (a load of the table at H = 256).  The offsets are
+  // additive: H / R1 = 64 is a multiple of 16, and j % 16 = b1 % 8 leaves
+  // room for 8 r % 16 below 16.
+  __device__ __forceinline__ explicit ZwMid(int b) {
+#pragma unroll
+    for (int i = 0; i < C1; ++i) {
+      const int b1 = H == 256 ? (int)kZwMid256[32 * i + b] : b + ZW<H>::LPR * i;
+      k[i] = b1 & 7;
+      ld[i] = zw_slot<H>(b1);
+      st[i] = zw_slot<H>((b1 - k[i]) * R1 + k[i]);
+    }
+  }
+};
+
 // The three stages of one H-point transform (INV: exp(+2 pi i nk/H)).  On
 // entry v[r] holds position b + (H/8) r of the lane's row, on exit output
-// b + (H/8) r.  xch is the row's exchange buffer; the warp must call this
-// converged.  Returns with the exchange buffer free for the next transform.
+// b + (H/8) r.  xch is the row's exchange buffer; mid the lane's middle-stage
+// butterflies; the warp must call this converged.  Returns with the exchange
+// buffer free for the next transform.
 template <int H, bool INV>
-__device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const float2* __restrict__ tws, int b) {
+__device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const float2* __restrict__ tws, int b,
+                                             const ZwMid<H>& mid) {
   using Z = ZW<H>;
   DFT<8, INV, float2>::run(v);  // stage 0 (P = 1): outputs 8b + r
 #pragma unroll
@@ -84,16 +119,16 @@ __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const 
   if constexpr (Z::R1 > 1) {
     constexpr int R1 = Z::R1, NB1 = H / R1, C1 = 8 / R1;
     float2 u[C1][R1];
+    static_assert(NB1 % 16 == 0, "additive exchange offsets");
 #pragma unroll
     for (int i = 0; i < C1; ++i) {
-      const int b1 = b + Z::LPR * i;
 #pragma unroll
-      for (int r = 0; r < R1; ++r) u[i][r] = xch[zw_slot<H>(b1 + NB1 * r)];
+      for (int r = 0; r < R1; ++r) u[i][r] = xch[mid.ld[i] + zw_slot<H>(NB1 * r)];
     }
     __syncwarp();
 #pragma unroll
     for (int i = 0; i < C1; ++i) {
-      const int b1 = b + Z::LPR * i, k = b1 & 7;
+      const int k = mid.k[i];
 #pragma unroll
       for (int r = 1; r < R1; ++r) {
         float2 w = tws[Z::TW1 + (r - 1) * 8 + k];
@@ -101,9 +136,8 @@ __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const 
         u[i][r] = cmul(u[i][r], w);
       }
       DFT<R1, INV, float2>::run(u[i]);
-      const int j = (b1 - k) * R1 + k;
 #pragma unroll
-      for (int r = 0; r < R1; ++r) xch[zw_slot<H>(j + 8 * r)] = u[i][r];
+      for (int r = 0; r < R1; ++r) xch[mid.st[i] + zw_slot<H>(8 * r)] = u[i][r];
     }
     __syncwarp();
   }
