@@ -92,7 +92,10 @@ struct Path {  // one code path: 0 = general (full layout), 1 = dealiased (2/3 b
   Buf t6, u6, U, ACC, S, D, partial, coef;
   Buf FEXT;  // external force held over a call (compact layout), see hit_rollout_forced
   int p3_blocks = 0, gather_blocks = 0;
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};  // [0]: last step, [1]: step that prepares the next one
+  // the rollout graph: a device-side while loop over the steps that prepare
+  // the next one, then the last step (see build_rollout_graph)
+  cudaGraphExec_t exec = nullptr;
+  Buf loop;  // int64 count of the loop's remaining steps
   GraphKey key{};
   bool key_valid = false;
 };
@@ -473,6 +476,76 @@ int rhs_impl(hit_plan* p, const void* u_hat, const hit_params* pr, void* du, con
   return HIT_OK;
 }
 
+// Loop control of the rollout graph: k_loop_set (launched on the caller's
+// stream before the graph) stores the count of loop steps, k_loop_arm (the
+// graph's first node) opens the while node when it is positive, and
+// k_loop_next (the last node of the loop body) counts one step down and
+// closes the loop at zero.
+__global__ void k_loop_set(long long* left, long long n) { *left = n; }
+__global__ void k_loop_arm(cudaGraphConditionalHandle h, const long long* left) {
+  cudaGraphSetConditional(h, *left > 0 ? 1u : 0u);
+}
+__global__ void k_loop_next(cudaGraphConditionalHandle h, long long* left) {
+  const long long v = *left - 1;
+  *left = v;
+  cudaGraphSetConditional(h, v > 0 ? 1u : 0u);
+}
+
+// The whole rollout of nsteps >= 1 steps from the x-inverse of U as one graph:
+//   k_loop_arm -> while (left > 0) { step that ends with the next step's
+//   x-inverse; k_loop_next } -> last step.
+// The loop count lives in device memory (P.loop), so one instantiated graph
+// serves every nsteps: the lax.scan of integrators.py:41-53 without a host
+// launch per step.
+template <typename T>
+int build_rollout_graph(hit_plan* p, Path& P, const Scalars& s, double dt, const V2<T>* fext,
+                        cudaGraphExec_t* exec) {
+  int rc;
+  cudaGraph_t g = nullptr;
+  HIT_CK(cudaGraphCreate(&g, 0));
+  struct Owner {
+    cudaGraph_t g;
+    ~Owner() { cudaGraphDestroy(g); }
+  } own{g};
+  cudaGraphConditionalHandle h;
+  HIT_CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  long long* left = static_cast<long long*>(P.loop.p);
+  cudaGraphNode_t arm = nullptr, loop = nullptr;
+  {
+    void* args[] = {&h, &left};
+    cudaKernelNodeParams kp{};
+    kp.func = reinterpret_cast<void*>(&k_loop_arm);
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = args;
+    HIT_CK(cudaGraphAddKernelNode(&arm, g, nullptr, 0, &kp));
+  }
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  HIT_CK(cudaGraphAddNode(&loop, g, &arm, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  // loop body: one step that prepares the next, then the count
+  HIT_CK(cudaStreamBeginCaptureToGraph(p->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  rc = enqueue_step<T>(p, P, s, dt, true, fext, p->cap);
+  if (!rc) k_loop_next<<<1, 1, 0, p->cap>>>(h, left);
+  cudaGraph_t got = nullptr;
+  cudaError_t e = cudaStreamEndCapture(p->cap, &got);
+  if (rc) return rc;
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "rollout loop body capture");
+  // after the loop: the last step
+  HIT_CK(cudaStreamBeginCaptureToGraph(p->cap, g, &loop, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+  rc = enqueue_step<T>(p, P, s, dt, false, fext, p->cap);
+  e = cudaStreamEndCapture(p->cap, &got);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "rollout last-step capture");
+  HIT_CK(cudaGraphInstantiate(exec, g, 0));
+  return HIT_OK;
+}
+
 template <typename T>
 int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, void* out,
                  const void* fext, cudaStream_t st) {
@@ -493,32 +566,19 @@ int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
       if ((rc = enqueue_step<T>(p, P, s, dt, i + 1 < nsteps, fext ? vp<T>(P.FEXT) : nullptr, st))) return rc;
   } else if (nsteps > 0) {
     const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing, s.ifrk, fext ? 1 : 0};
+    if ((rc = ensure(P.loop, sizeof(long long)))) return rc;
     if (!P.key_valid || !(P.key == key)) {
-      for (cudaGraphExec_t& ex : P.exec) {
-        if (ex) cudaGraphExecDestroy(ex);
-        ex = nullptr;
-      }
+      if (P.exec) cudaGraphExecDestroy(P.exec);
+      P.exec = nullptr;
       P.key_valid = false;
-      for (int fused = 0; fused < 2; ++fused) {
-        HIT_CK(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
-        rc = enqueue_step<T>(p, P, s, dt, fused == 1, fext ? vp<T>(P.FEXT) : nullptr, p->cap);
-        cudaGraph_t graph = nullptr;
-        cudaError_t e = cudaStreamEndCapture(p->cap, &graph);
-        if (rc) {
-          if (graph) cudaGraphDestroy(graph);
-          return rc;
-        }
-        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&P.exec[fused], graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
-      }
+      if ((rc = build_rollout_graph<T>(p, P, s, dt, fext ? vp<T>(P.FEXT) : nullptr, &P.exec))) return rc;
       P.key = key;
       P.key_valid = true;
     }
+    k_loop_set<<<1, 1, 0, st>>>(static_cast<long long*>(P.loop.p), (long long)(nsteps - 1));
+    HIT_CK(cudaGetLastError());
     if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
-    for (int64_t i = 0; i + 1 < nsteps; ++i) HIT_CK(cudaGraphLaunch(P.exec[1], st));
-    HIT_CK(cudaGraphLaunch(P.exec[0], st));
+    HIT_CK(cudaGraphLaunch(P.exec, st));
   }
   HIT_CK(launch_scatter<T>(vp<T>(P.U), static_cast<V2<T>*>(out), P.g, st));
   return HIT_OK;
@@ -1040,8 +1100,8 @@ int hit_plan_destroy(hit_plan* p) {
   if (!p) return HIT_OK;
   DeviceGuard dg(p->device);
   for (Path& P : p->path) {
-    for (cudaGraphExec_t ex : P.exec)
-      if (ex) cudaGraphExecDestroy(ex);
+    if (P.exec) cudaGraphExecDestroy(P.exec);
+    release(P.loop);
     release(P.t6);
     release(P.u6);
     release(P.U);
