@@ -1,9 +1,10 @@
 """Time integration (reference: src/hit3d/integrators.py).
 
 ``rk4_step`` and ``rollout`` with the package's own RHS and a built-in
-forcing run entirely in the fused kernels: the rollout replays a CUDA graph
-of one RK4 step ``nsteps`` times on the current stream with no host
-synchronisation (the replacement for the jitted ``lax.scan``).  Any other
+forcing run entirely in the fused kernels: the rollout is one launch of a CUDA
+graph whose while node loops over the ``nsteps`` steps on the device, on the
+current stream with no host synchronisation (the replacement for the jitted
+``lax.scan``).  Any other
 ``rhs`` callable is integrated by composing its calls with the reference's
 stage algebra.  ``evolve`` is the host loop over rollout segments with
 callbacks (reference interface: integrators.py:56-109).
