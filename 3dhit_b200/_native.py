@@ -81,6 +81,7 @@ SIGNATURES = {
     "hit_velocity_gradients_vjp": (_i, [_vp, _vp, _vp, _vp]),
     "hit_mlp_vjp": (_i, [_vp, _vp, _vp, _i64, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hit_rollout_forced": (_i, [_vp, _vp, _PP, _vp, _d, _i64, _d, _vp, _vp]),
+    "hit_les_rollout": (_i, [_vp, _vp, _PP, _vp, _d, _i64, _vp, _vp, _vp]),
     "hit_profile_rollout": (_i, [_vp, _vp, _PP, _d, _i64, _vp, _vp, _vp, _vp]),
     "hit_rhs_vjp": (_i, [_vp, _vp, _PP, _d, _vp, _vp, _vp, _vp]),
     "hit_rk4_step_vjp": (_i, [_vp, _vp, _PP, _d, _d, _vp, _vp, _vp, _vp]),

@@ -231,6 +231,46 @@ __device__ __forceinline__ void p1_body(SRC&& comp, V2<T>* A, V2<T>* B, int j, i
   sync();
 }
 
+// x-inverse for the fused LES stage: u and the nine velocity gradients
+// g_ij = d_j u_i (spectral i k_j u_i, in the order 3 i + j of
+// hit_velocity_gradients) of one (ky row, z tile), 12 outputs (u_x, u_y, u_z,
+// g_00 .. g_22).  ky and kz are constant along an x column, so six transforms
+// (u_i and kx u_i) give all of them; the z pass forms w from the gradients.
+template <typename T, int N, int W, int NTH, class SRC>
+__device__ __forceinline__ void p1les_body(SRC&& comp, V2<T>* A, V2<T>* B, int j, int z0, const Geom& g,
+                                           const KTab<T>& kt, const V2<T>* tws, V2<T>* t12, long long t_c,
+                                           long long t_x) {
+  const int fy = full_pos(j, g.hy, g.My, g.Ny);
+  const T ky = kt.ky[fy];
+  V2<T>* out = t12 + (long long)j * g.Mzp + z0;
+  constexpr int NS = fft_nstages(N);
+  auto kz_of = [&](int col) {
+    const int z = z0 + col;
+    return z < g.Nzh ? kt.kz[z] : T(0);
+  };
+  auto put = [&](int q, int pos, int col, V2<T> v) { out[q * t_c + (long long)pos * t_x + col] = v; };
+  auto sync = [&]() {
+    if constexpr (NS % 2 == 0) __syncthreads();
+  };
+#pragma unroll 1
+  for (int i = 0; i < 3; ++i) {
+    // u_i -> u_i, g_i1 = i ky u_i, g_i2 = i kz u_i
+    fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
+        A, B, tws, [&](int pos, int col, int r) { return comp(i, pos, col, r); },
+        [&](int pos, int col, V2<T> v) {
+          put(i, pos, col, v);
+          put(3 + 3 * i + 1, pos, col, cmul_i(cscale(v, ky)));
+          put(3 + 3 * i + 2, pos, col, cmul_i(cscale(v, kz_of(col))));
+        });
+    sync();
+    // kx u_i -> g_i0
+    fft_io<T, N, W, NTH, TileAddr<N, W>, true>(
+        A, B, tws, [&](int pos, int col, int r) { return cscale(comp(i, pos, col, r), kt.kx[pos]); },
+        [&](int pos, int col, V2<T> v) { put(3 + 3 * i, pos, col, cmul_i(v)); });
+    sync();
+  }
+}
+
 template <typename T, int N, int W, int NTH>
 __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -265,8 +305,12 @@ __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
         S[c * NW + full_pos(i, g.hx, g.Mx, N) * W + col] = src[c * a.s_c + (long long)i * a.s_x + col];
       }
     __syncthreads();
-    p1_body<T, N, W, NTH>([&](int c, int pos, int col, int) { return S[c * NW + pos * W + col]; }, A, B, j, z0, g,
-                          a.k, tws, a.t6, a.t_c, a.t_x);
+    if (a.les)
+      p1les_body<T, N, W, NTH>([&](int c, int pos, int col, int) { return S[c * NW + pos * W + col]; }, A, B, j, z0,
+                               g, a.k, tws, a.t6, a.t_c, a.t_x);
+    else
+      p1_body<T, N, W, NTH>([&](int c, int pos, int col, int) { return S[c * NW + pos * W + col]; }, A, B, j, z0, g,
+                            a.k, tws, a.t6, a.t_c, a.t_x);
   }
 }
 
@@ -277,6 +321,12 @@ __global__ void __launch_bounds__(NTH) k_p1(P1Args<T> a, int nzt, int ntiles) {
 // never pass through shared memory.
 template <int N, int W, int NTH> __host__ __device__ constexpr bool p3_in_regs() {
   return N >= 64 && fft_radix(N, 0) == 8 && fft_radix(N, fft_nstages(N) - 1) == 8 && (N / 8) * W == NTH;
+}
+// Instantiations that run the fused LES stage (float32, shared-memory mode,
+// columns of at most 256 points): their nl tile holds 3 more components, the
+// divergence k_j tau_hat_ij of the SGS stress.
+template <typename T, int N, int W, int NTH> __host__ __device__ constexpr bool p3_les() {
+  return std::is_same<T, float>::value && !p3_in_regs<N, W, NTH>() && N <= 256;
 }
 
 // State rows of one mode for the epilogue: us = stage input (u for stages
@@ -456,6 +506,7 @@ template <typename T, int N, int W, int NTH>
 __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, const V2<T>* tws, V2<T>* F, double* red,
                                         int j, int z0, int tile, V2<T>* stg, int nzt, int ntiles) {
   constexpr bool REGS = p3_in_regs<N, W, NTH>();
+  constexpr bool LES = p3_les<T, N, W, NTH>();
   const Geom& g = a.g;
   const int MW = g.Mx * W;
   constexpr int VPC = 16 / sizeof(V2<T>);
@@ -526,7 +577,7 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
     fft_io<T, N, W, NTH, TileAddr<N, W>, false>(
         A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; }, nl_store(c),
         [&]() {
-          if (c < 2) {
+          if (c < 2 || (LES && a.les)) {
             prefetch(tile, c + 1, stg);
           } else {
             if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, 0, stg);
@@ -534,6 +585,42 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
             stage_pass(1);
           }
         });
+  }
+  if constexpr (LES) {
+    // fused LES stage: x-forward of the six stress components (xx, yy, zz,
+    // xy, xz, yz), accumulated into s_i = k_j tau_hat_ij in F[3..5]
+    // (the first contribution of each s_i writes, the later ones add)
+    if (a.les) {
+      const T kyl = a.k.ky[full_pos(j, g.hy, g.My, g.Ny)];
+#pragma unroll 1
+      for (int c = 3; c < 9; ++c) {
+        cp_async_wait_all();
+        __syncthreads();
+        fft_io<T, N, W, NTH, TileAddr<N, W>, false>(
+            A, B, tws, [&](int pos, int col) { return stg[pos * W + col]; },
+            [&](int pos, int col, V2<T> v) {
+              const int row = compact_row(pos, g.hx, g.Mx, N);
+              if (row < 0) return;
+              const int z = z0 + col;
+              const T kx = a.k.kx[pos], kz = z < g.Mz ? a.k.kz[z] : T(0);
+              V2<T>* s0 = F + 3 * MW + row * W + col;
+              V2<T>* s1 = s0 + MW;
+              V2<T>* s2 = s1 + MW;
+              switch (c) {
+                case 3: *s0 = cscale(v, kx); break;
+                case 4: *s1 = cscale(v, kyl); break;
+                case 5: *s2 = cscale(v, kz); break;
+                case 6: *s0 = cadd(*s0, cscale(v, kyl)); *s1 = cadd(*s1, cscale(v, kx)); break;
+                case 7: *s0 = cadd(*s0, cscale(v, kz)); *s2 = cadd(*s2, cscale(v, kx)); break;
+                default: *s1 = cadd(*s1, cscale(v, kz)); *s2 = cadd(*s2, cscale(v, kyl)); break;
+              }
+            },
+            [&]() {
+              if (c < 8) prefetch(tile, c + 1, stg);
+              else if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, 0, stg);
+            });
+      }
+    }
   }
   if constexpr (!REGS) __syncthreads();  // F complete
 
@@ -599,6 +686,16 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
         V2<T> ns[3] = {czero<T>(), czero<T>(), czero<T>()};
         if (ok[h]) {
           V2<T> du[3] = {F[e], F[MW + e], F[2 * MW + e]};
+          if constexpr (LES) {
+            if (a.les) {  // f = -i k_j tau_hat_ij: added here, held for the later stages
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                const V2<T> fc = cmul_mi(F[(3 + c) * MW + e]);
+                du[c] = cadd(du[c], fc);
+                a.fext_out[c * a.c_c + idx[h]] = fc;
+              }
+            }
+          }
           p3_point(a, full_pos(i, g.hx, g.Mx, N), fy, z0 + col, ky, __ldg(a.k.kz + z0 + col), cf, idx[h], du, us[h],
                    ac[h], uu[h], ns, sE, sO, sB);
         }
@@ -623,6 +720,17 @@ __device__ __forceinline__ void p3_tile(const P3Args<T>& a, V2<T>* A, V2<T>* B, 
                             a.t6_x);
   } else {
     __syncthreads();  // F complete; A/B free for the next tile or the fused x-inverse
+    if constexpr (LES) {
+      if (a.fuse_p1 == 2) {  // the next stage is a fused LES stage
+        p1les_body<T, N, W, NTH>(
+            [&](int c, int pos, int col, int) {
+              const int row = compact_row(pos, g.hx, g.Mx, N);
+              return row >= 0 ? F[c * MW + row * W + col] : czero<T>();
+            },
+            A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x);
+        return;
+      }
+    }
     if (a.fuse_p1)
       p1_body<T, N, W, NTH>(
           [&](int c, int pos, int col, int) {
@@ -958,7 +1066,8 @@ template <typename T, int N> size_t p1_smem(int W) {
   return sizeof(V2<T>) * ((size_t)2 * skew8_slots(N, W) + 3 * N * W + tw_slots_even<N>());
 }
 template <typename T, int N, int W, int NTH> size_t p3_smem(int Mx) {
-  const size_t f = p3_in_regs<N, W, NTH>() ? (size_t)3 * p3_ring_slot<N, W>() : (size_t)3 * Mx * W;
+  const size_t f = p3_in_regs<N, W, NTH>() ? (size_t)3 * p3_ring_slot<N, W>()
+                                           : (size_t)(p3_les<T, N, W, NTH>() ? 6 : 3) * Mx * W;
   return sizeof(V2<T>) * ((size_t)2 * skew8_slots(N, W) + N * W + tw_slots_even<N>() + f);
 }
 template <typename T, int N, int W, bool PF> constexpr size_t axis_smem() {

@@ -24,55 +24,15 @@
 #include <algorithm>
 
 #include "kernels.h"
+#include "mlp_core.cuh"
 #include "tc_common.cuh"
 
 namespace hit {
 
+using namespace mlp;
+
 namespace {
 constexpr int MLP_WAIT = 1 << 22;
-
-// GELU in its tanh form (Hendrycks and Gimpel, 2016),
-//   gelu(x) = x/2 (1 + tanh(u)),  u = sqrt(2/pi) (x + 0.044715 x^3),
-// with the hardware tanh (tanh.approx.f32, relative error about 2^-11, below
-// the bf16 rounding the activations get next), and its exact derivative
-//   gelu'(x) = (1 + t)/2 + x/2 (1 - t^2) sqrt(2/pi) (1 + 3 * 0.044715 x^2).
-__device__ __forceinline__ float tanh_hw(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float gelu(float x) {
-  const float t = tanh_hw(x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f));
-  const float h = 0.5f * x;
-  return fmaf(h, t, h);
-}
-__device__ __forceinline__ float gelu_d(float x) {
-  const float t = tanh_hw(x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f));
-  const float du = fmaf(0.10703222440890037f, x * x, 0.7978845608028654f);
-  return fmaf(0.5f * x * fmaf(-t, t, 1.f), du, 0.5f * (1.f + t));
-}
-
-// Copy a row-major bf16 matrix [R][KC] into the K-major core-matrix layout.
-__device__ __forceinline__ void load_kmajor(unsigned char* dst, const __nv_bfloat16* __restrict__ src, int R, int KC) {
-  for (int e = threadIdx.x; e < R * (KC / 8); e += blockDim.x) {
-    const int r = e / (KC / 8), c8 = e % (KC / 8);
-    *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, c8 * 8, KC)) =
-        *reinterpret_cast<const uint4*>(src + (long long)r * KC + c8 * 8);
-  }
-}
-
-// This thread's row (point) of a K-major tile with KC columns from n floats
-// (columns past n are zero).
-template <int KC>
-__device__ __forceinline__ void store_row(unsigned char* tile, int row, const float* v, int n) {
-#pragma unroll
-  for (int c8 = 0; c8 < KC / 8; ++c8) {
-    __align__(16) __nv_bfloat16 h[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16_rn(c8 * 8 + i < n ? v[c8 * 8 + i] : 0.f);
-    *reinterpret_cast<uint4*>(tile + tc::kmajor_off(row, c8 * 8, KC)) = *reinterpret_cast<const uint4*>(h);
-  }
-}
 }  // namespace
 
 template <bool TRAIN> struct MlpSmem {

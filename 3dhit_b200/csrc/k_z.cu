@@ -15,10 +15,13 @@
 // first stage forms u x w from them; its last stage leaves the spectrum in
 // shared memory for the r2c post-processing, which writes the three products
 // over the first three input components of the same rows.
+#include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "fft_core.cuh"
 #include "kernels.h"
+#include "mlp_core.cuh"
 #include "tma.cuh"
 #include "zwarp.cuh"
 
@@ -209,6 +212,143 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
     __syncthreads();  // buf is rewritten by the next group
   }
   cp_async_wait_all();
+}
+
+// k_zles: the z pass of the fused LES stage (float32, Nz = 2H in {32, 64,
+// 128}).  A CTA of 128 threads takes RB = 128 / Nz (x, y) rows at a time:
+//   * c2r of u and the nine velocity gradients g_ij = d_j u_i (12 rows each,
+//     staged by bulk TMA copies as in k_zcross);
+//   * thread t then owns physical point t of the group (row t / Nz, z = t % Nz):
+//     w = (g_21 - g_12, g_02 - g_20, g_10 - g_01), u x w
+//     (src/hit3d/navierstokes.py:73-86), and the closure MLP on the tensor cores
+//     (mlp::infer_tile: the nine gradients in physical units in, the six SGS
+//     stresses out; thread t is TMEM lane t of the 128-point tile);
+//   * r2c of the three products and the six stresses, written over the first
+//     nine input rows of each (x, y) row.
+// The unnormalised inverse transforms leave every physical value times
+// Nx Ny Nz: the gradients are scaled back for the MLP, and the products take
+// (1/(Nx Ny Nz))^2 / 2, the stresses 1/2 (the r2c post-processing's halving).
+constexpr int ZLES_MMA_WAIT = 1 << 22;  // mbarrier polls before an MMA wait gives up
+
+template <int H>
+__global__ void __launch_bounds__(128) k_zles(ZLesArgs a) {
+  constexpr int NZ = 2 * H, RB = 128 / NZ, NTZ = 128;
+  using AD = SkewAddr<skew_ld(H)>;
+  constexpr int RS = z_row_cap<H>();
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  mlp::InferSmem& M = *reinterpret_cast<mlp::InferSmem*>(smem_raw);
+  float2* buf = reinterpret_cast<float2*>(smem_raw + (sizeof(mlp::InferSmem) + 127) / 128 * 128);
+  float2* tws = buf + 12 * RB * AD::LD;
+  const float2* twz = tws + tw_size<true>(H);
+  float2* raw = tws + z_tw_slots<H>();  // 12 RB staged rows of RS entries
+  __shared__ __align__(8) uint64_t zbar;
+  const int Mzp = a.Mzp, Mz = a.Mz;
+  for (int e = threadIdx.x; e < 12 * RB * RS; e += NTZ)
+    if (e % RS >= Mzp) raw[e] = make_float2(0.f, 0.f);
+  mlp::infer_setup(M, a.w1t, a.w2t, a.w3t, a.w4t, a.b2, a.b3, a.b4);
+  const uint32_t mb = tma::smem_u32(&zbar);
+  if (threadIdx.x == 0) tma::mbar_init(mb, 1);
+  tma::fence_async_smem();
+  fill_z_twiddles<float, H, NTZ>(tws, a.tw);  // ends with __syncthreads
+  tc::fence_after_sync();
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  const int ngroups = (a.nrows + RB - 1) / RB;
+  auto prefetch = [&](int grp) {
+    if (threadIdx.x < 32) {
+      const long long r0 = (long long)grp * RB;
+      const int nin = (int)(a.nrows - r0 < RB ? a.nrows - r0 : RB);
+      const uint32_t bytes = (uint32_t)(Mzp * sizeof(float2));
+      if (threadIdx.x == 0) tma::mbar_expect_tx(mb, 12u * nin * bytes);
+      __syncwarp();
+      for (int col = threadIdx.x; col < 12 * RB; col += 32) {
+        const int q = col / RB, lr = col % RB;
+        if (lr < nin) tma::load_bytes(raw + col * RS, a.buf + q * a.c_stride + (r0 + lr) * Mzp, bytes, mb);
+      }
+    }
+  };
+  const int wait_limit = g_z_wait_limit;
+  pdl_wait();
+  pdl_trigger();
+  int grp = blockIdx.x;
+  if (grp < ngroups) prefetch(grp);
+  uint32_t phase = 0, mphase = 0;
+  bool ok = true;
+  for (; grp < ngroups && ok; grp += gridDim.x) {
+    const long long row0 = (long long)grp * RB;
+    {
+      const bool landed = __syncthreads_and(tma::mbar_wait(mb, phase, wait_limit)) != 0;
+      phase ^= 1;
+      if (!landed) {
+        if (threadIdx.x == 0) atomicExch(&g_z_timeout, 1);
+        tma::mbar_wait(mb, phase ^ 1, Z_WAIT);  // the copies in flight, once more with a limit
+        break;
+      }
+    }
+    const int nxt = grp + gridDim.x;
+    fft_ip<float, H, 12 * RB, NTZ, AD, true>(
+        buf, tws,
+        [&](int k, int col) {
+          const float2* row = raw + col * RS;
+          float2 X = row[k];
+          float2 Y = row[H - k];
+          if (k == 0) {
+            X.y = 0.f;
+            Y.y = 0.f;
+          }
+          Y.y = -Y.y;
+          const float2 sm = cadd(X, Y), df = csub(X, Y);
+          float2 w = twz[k];
+          w.y = -w.y;
+          return cadd(sm, cmul_i(cmul(w, df)));
+        },
+        [&](int m, int col, float2 v) { buf[AD::at(m, col)] = v; },
+        [&]() {
+          if (nxt < ngroups) prefetch(nxt);
+        });
+    // this thread's physical point
+    const int lr = threadIdx.x / NZ, zp = threadIdx.x % NZ, m = zp >> 1, hf = zp & 1;
+    const float* bf = reinterpret_cast<const float*>(buf);
+    auto val = [&](int q) { return bf[2 * AD::at(m, q * RB + lr) + hf]; };
+    float u[3], gr[9], gp[9];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) u[q] = val(q);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      gr[q] = val(3 + q);
+      gp[q] = gr[q] * a.scale;
+    }
+    const float w[3] = {gr[7] - gr[5], gr[2] - gr[6], gr[3] - gr[1]};
+    const float s2 = 0.5f * a.scale * a.scale;
+    float nl[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int c1 = c == 2 ? 0 : c + 1, c2 = c == 0 ? 2 : c - 1;  // (1,2), (2,0), (0,1)
+      nl[c] = (u[c1] * w[c2] - u[c2] * w[c1]) * s2;
+    }
+    float tau[6];
+    mlp::infer_tile(M, gp, tau, mphase, ok, ZLES_MMA_WAIT);  // all threads; its first MMA syncs the block
+    float* bw = reinterpret_cast<float*>(buf);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) bw[2 * AD::at(m, c * RB + lr) + hf] = nl[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) bw[2 * AD::at(m, (3 + c) * RB + lr) + hf] = 0.5f * tau[c];
+    __syncthreads();
+    fft_ip<float, H, 9 * RB, NTZ, AD, false>(
+        buf, tws, [&](int mm, int col) { return buf[AD::at(mm, col)]; },
+        [&](int k, int col, float2 v) { buf[AD::at(k, col)] = v; });
+    for (int col = warp; col < 9 * RB; col += NTZ / 32) {
+      const int q = col / RB, rr = col % RB;
+      if (row0 + rr < a.nrows) {
+        float2* out = a.buf + q * a.c_stride + (row0 + rr) * Mzp;
+        for (int k = lane; k < Mzp; k += 32)
+          out[k] = k < Mz ? r2c_post<float, false>([&](int i) { return buf[AD::at(i, col)]; }, k, H, twz)
+                          : make_float2(0.f, 0.f);
+      }
+    }
+    __syncthreads();  // buf is rewritten by the next group
+  }
+  if (!ok && threadIdx.x == 0) atomicExch(a.err, 1);
+  mlp::infer_teardown(M);
 }
 
 // k_zwarp: the fused z pass of k_zcross (same inputs, outputs and arithmetic
@@ -588,6 +728,53 @@ template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, c
     constexpr int HH = decltype(hh)::value;
     return launch_zcross_v<T, HH, z_rows_per_block<HH>(), z_threads<HH>(), 4>(a, st);
   });
+}
+
+template <int HH> size_t zles_smem() {
+  using AD = SkewAddr<skew_ld(HH)>;
+  constexpr int RB = 128 / (2 * HH);
+  return (sizeof(mlp::InferSmem) + 127) / 128 * 128 +
+         sizeof(float2) * (12 * RB * AD::LD + z_tw_slots<HH>() + 12 * RB * z_row_cap<HH>());
+}
+
+template <int HH> cudaError_t launch_zles_v(const ZLesArgs& a, cudaStream_t st) {
+  static PerDevice ready, cache;
+  constexpr int RB = 128 / (2 * HH);
+  const size_t smem = zles_smem<HH>();
+  cudaError_t e = once_per_device(ready, [&] {
+    cudaError_t r = cudaFuncSetAttribute(k_zles<HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (r != cudaSuccess) return r;
+    return cudaFuncSetAttribute(k_zles<HH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
+  });
+  if (e != cudaSuccess) return e;
+  // resident CTAs from the SM's shared memory (the occupancy query counts one
+  // CTA per SM for kernels that allocate tensor memory), at most 8 per SM (8 x
+  // 64 TMEM columns)
+  std::atomic<int>* slot = cache.here();
+  int wave = slot ? slot->load(std::memory_order_relaxed) : 0;
+  if (wave == 0) {
+    int dev = 0, sms = 0, smem_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+      return e;
+    const int per_sm = std::max(1, std::min((int)(smem_sm / (smem + 1024 + 64)), 8));
+    wave = per_sm * std::max(sms, 1);
+    if (slot) slot->store(wave, std::memory_order_relaxed);
+  }
+  const int groups = (a.nrows + RB - 1) / RB;
+  return launch_pdl(k_zles<HH>, std::max(1, std::min(groups, wave)), 128, smem, st, a);
+}
+
+bool zles_supported(int Nz) { return Nz == 32 || Nz == 64 || Nz == 128; }
+
+cudaError_t launch_zles(int H, const ZLesArgs& a, cudaStream_t st) {
+  if (a.Mzp % 8 || a.Mzp > (H + 1 + 7) / 8 * 8) return cudaErrorInvalidValue;
+  if (H == 16) return launch_zles_v<16>(a, st);
+  if (H == 32) return launch_zles_v<32>(a, st);
+  if (H == 64) return launch_zles_v<64>(a, st);
+  return cudaErrorInvalidValue;
 }
 
 template <typename T, bool C2R> cudaError_t launch_zreal(int H, const ZRealArgs<T>& a, int ncomp, cudaStream_t st) {

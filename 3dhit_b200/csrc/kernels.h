@@ -62,6 +62,7 @@ template <typename T> struct AxisArgs {
 template <typename T> struct P1Args {
   const V2<T>* s;   // (3, Mx, My, Mzp)
   long long s_c, s_x;
+  int les;          // 1: 12 outputs, u and the velocity gradients (see p1les_body)
   V2<T>* t6;        // (6, Nx, My, Mzp)
   long long t_c, t_x;
   Geom g;
@@ -97,6 +98,12 @@ template <typename T> struct P3Args {
   double* partial;     // per-block (3 per block) sums of the new stage input
   const V2<T>* fext;   // optional external force (compact layout, index o like u),
                        // added to the nonlinear term before the mask and projection
+  // fused LES stage (shared-memory mode only): t3 holds 9 x-physical fields,
+  // u x w then the SGS stress tau (xx, yy, zz, xy, xz, yz); the epilogue forms
+  // f = -i k_j tau_hat_ij, adds it to the nonlinear term and stores it at
+  // fext_out (compact layout) for the step's later stages
+  int les;
+  V2<T>* fext_out;
 };
 
 // Fused z pass of the RHS: per (x, y) row, c2r of 6 components, u x w,
@@ -108,6 +115,23 @@ template <typename T> struct ZCrossArgs {
   T scale;     // 1/(Nx Ny Nz)
   const V2<T>* tw;
 };
+
+// z pass of the fused LES stage (k_zles, float32): per (x, y) row, c2r of u
+// and the nine velocity gradients, u x w and the closure MLP per physical
+// point, r2c of the three products and the six SGS stresses (xx, yy, zz,
+// xy, xz, yz), written over the first nine of the twelve input rows.
+struct ZLesArgs {
+  float2* buf;  // (12, Nx, Ny, Mzp)
+  long long c_stride;
+  int nrows, Mz, Mzp;
+  float scale;  // 1/(Nx Ny Nz)
+  const float2* tw;
+  const __nv_bfloat16 *w1t, *w2t, *w3t, *w4t;  // the MLP's forward weights (hit_mlp_weights)
+  const float *b2, *b3, *b4;
+  int* err;     // set when an MMA completion wait gave up
+};
+cudaError_t launch_zles(int H, const ZLesArgs& a, cudaStream_t st);
+bool zles_supported(int Nz);
 
 // Plain z c2r / r2c for to_physical / to_spectral.
 template <typename T> struct ZRealArgs {

@@ -97,6 +97,14 @@ struct Path {  // one code path: 0 = general (full layout), 1 = dealiased (2/3 b
   cudaGraphExec_t exec = nullptr;
   Buf loop;  // int64 count of the loop's remaining steps
   GraphKey key{};
+  // fused LES (hit_les_rollout): 12-field x- and y-pass buffers, its rollout
+  // graph and the key it was built for (parameters and MLP weights)
+  Buf t12, u12;
+  cudaGraphExec_t les_exec = nullptr;
+  GraphKey les_key{};
+  hit_mlp_weights les_w{};
+  int* les_err = nullptr;
+  bool les_key_valid = false;
   bool key_valid = false;
 };
 
@@ -285,13 +293,14 @@ template <typename T> int gather_state(hit_plan* p, Path& P, const void* u_hat, 
   return HIT_OK;
 }
 
-template <typename T> int launch_p1_of(hit_plan* p, Path& P, const V2<T>* src, cudaStream_t st) {
+template <typename T> int launch_p1_of(hit_plan* p, Path& P, const V2<T>* src, cudaStream_t st, bool les = false) {
   const Geom& g = P.g;
   P1Args<T> a{};
   a.s = src;
   a.s_c = (long long)g.Mx * g.My * g.Mzp;
   a.s_x = (long long)g.My * g.Mzp;
-  a.t6 = vp<T>(P.t6);
+  a.les = les ? 1 : 0;
+  a.t6 = vp<T>(les ? P.t12 : P.t6);
   a.t_c = (long long)g.Nx * g.My * g.Mzp;
   a.t_x = (long long)g.My * g.Mzp;
   a.g = g;
@@ -352,12 +361,77 @@ template <typename T> int launch_p2(hit_plan* p, Path& P, cudaStream_t st, Prof*
   return HIT_OK;
 }
 
+// P2 of the fused LES stage (float32): T12 -> U12 (y-inverse of u and the
+// nine velocity gradients), the LES z pass in place on U12 (u x w, the
+// closure MLP, r2c of the products and the stresses), U12[0:9] -> T12[0:9]
+// (y-forward).
+int launch_p2_les(hit_plan* p, Path& P, const hit_mlp_weights& w, int* err, cudaStream_t st) {
+  const Geom& g = P.g;
+  const long long tc = (long long)g.Nx * g.My * g.Mzp, uc = (long long)g.Nx * g.Ny * g.Mzp;
+  const int Wy = axis_tile_w<float>(g.Ny);
+  AxisArgs<float> a{};
+  a.src = vp<float>(P.t12);
+  a.dst = vp<float>(P.u12);
+  a.s_c = tc;
+  a.s_a = g.Mzp;
+  a.s_o = (long long)g.My * g.Mzp;
+  a.d_c = uc;
+  a.d_a = g.Mzp;
+  a.d_o = (long long)g.Ny * g.Mzp;
+  a.Min = g.My;
+  a.hin = g.hy;
+  a.Mout = g.Ny;
+  a.hout = g.Ny / 2;
+  a.nz = g.Mzp;
+  a.tw = tw_of<float>(p);
+  HIT_CK(launch_axis<float>(g.Ny, true, a, g.Mzp / Wy, g.Nx, 12, st));
+  ZLesArgs z{};
+  z.buf = vp<float>(P.u12);
+  z.c_stride = uc;
+  z.nrows = g.Nx * g.Ny;
+  z.Mz = g.Mz;
+  z.Mzp = g.Mzp;
+  z.scale = (float)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
+  z.tw = tw_of<float>(p);
+  z.w1t = static_cast<const __nv_bfloat16*>(w.w1t);
+  z.w2t = static_cast<const __nv_bfloat16*>(w.w2t);
+  z.w3t = static_cast<const __nv_bfloat16*>(w.w3t);
+  z.w4t = static_cast<const __nv_bfloat16*>(w.w4t);
+  z.b2 = w.b2;
+  z.b3 = w.b3;
+  z.b4 = w.b4;
+  z.err = err;
+  HIT_CK(launch_zles(g.H, z, st));
+  AxisArgs<float> b{};
+  b.src = vp<float>(P.u12);
+  b.dst = vp<float>(P.t12);
+  b.s_c = uc;
+  b.s_a = g.Mzp;
+  b.s_o = (long long)g.Ny * g.Mzp;
+  b.d_c = tc;
+  b.d_a = g.Mzp;
+  b.d_o = (long long)g.My * g.Mzp;
+  b.Min = g.Ny;
+  b.hin = g.Ny / 2;
+  b.Mout = g.My;
+  b.hout = g.hy;
+  b.nz = g.Mzp;
+  b.tw = tw_of<float>(p);
+  HIT_CK(launch_axis<float>(g.Ny, false, b, g.Mzp / Wy, g.Nx, 9, st));
+  return HIT_OK;
+}
+
+// les_in: the fused LES stage (x-forward of T12's nine fields, the force
+// -i k_j tau_hat_ij added and stored in FEXT); les_next: the fused x-inverse
+// is the LES one (12 fields into T12), for a following fused LES stage.
 template <typename T>
 int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt, bool fuse, bool partial,
-                    const V2<T>* fext, cudaStream_t st) {
+                    const V2<T>* fext, cudaStream_t st, bool les_in = false, bool les_next = false) {
   const Geom& g = P.g;
   P3Args<T> a{};
-  a.t3 = vp<T>(P.t6);
+  a.t3 = vp<T>(les_in ? P.t12 : P.t6);
+  a.les = les_in ? 1 : 0;
+  a.fext_out = les_in ? vp<T>(P.FEXT) : nullptr;
   a.t_c = (long long)g.Nx * g.My * g.Mzp;
   a.t_x = (long long)g.My * g.Mzp;
   a.u = vp<T>(P.U);
@@ -366,14 +440,14 @@ int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt
   a.out = vp<T>(P.D);
   a.c_c = (long long)g.Mx * g.My * g.Mzp;
   a.c_x = (long long)g.My * g.Mzp;
-  a.t6 = vp<T>(P.t6);
+  a.t6 = vp<T>(fuse && les_next ? P.t12 : P.t6);
   a.t6_c = a.t_c;
   a.t6_x = a.t_x;
   a.g = g;
   a.k = ktab_of<T>(p);
   a.tw = tw_of<T>(p);
   a.stage = stage;
-  a.fuse_p1 = fuse ? 1 : 0;
+  a.fuse_p1 = fuse ? (les_next ? 2 : 1) : 0;
   a.ifrk = stage > 0 && s.ifrk ? 1 : 0;
   a.nu = a.ifrk ? (T)0 : (T)s.nu;
   a.nuh = (T)(0.5 * dt * s.nu);
@@ -404,6 +478,33 @@ int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, bool fuse_ne
     if ((rc = launch_p2<T>(p, P, st, pf))) return rc;
     TIMED(pf, 4, launch_p3_stage<T>(p, P, s, stage, dt, stage < 4 || fuse_next, red, fext, st));
     if (red) TIMED(pf, 5, launch_coef<T>(p, P, s, P.p3_blocks, st));
+  }
+  return HIT_OK;
+}
+
+// One RK4 step of the coarse LES with the learned closure fused into its
+// first stage (float32, dealiased path): stage 1 runs the LES passes (the
+// closure's force f = -i k_j tau_hat_ij from the step's initial state, added
+// to that stage's nonlinear term and stored in FEXT), stages 2-4 the plain
+// passes with f held (the scheme of hit_rollout_forced with the force of
+// hit_sgs_force).  Starts from the LES x-inverse of U in T12; with fuse_next
+// the last stage runs the next step's LES x-inverse.
+int enqueue_les_step(hit_plan* p, Path& P, const Scalars& s, double dt, bool fuse_next, const hit_mlp_weights& w,
+                     int* err, cudaStream_t st) {
+  int rc;
+  const bool red = needs_coef(s.forcing);
+  const float2* f = vp<float>(P.FEXT);
+  for (int stage = 1; stage <= 4; ++stage) {
+    if (stage == 1) {
+      if ((rc = launch_p2_les(p, P, w, err, st))) return rc;
+      if ((rc = launch_p3_stage<float>(p, P, s, 1, dt, true, red, nullptr, st, true, false))) return rc;
+    } else {
+      if ((rc = launch_p2<float>(p, P, st))) return rc;
+      if ((rc = launch_p3_stage<float>(p, P, s, stage, dt, stage < 4 || fuse_next, red, f, st, false,
+                                       stage == 4 && fuse_next)))
+        return rc;
+    }
+    if (red && (rc = launch_coef<float>(p, P, s, P.p3_blocks, st))) return rc;
   }
   return HIT_OK;
 }
@@ -491,15 +592,15 @@ __global__ void k_loop_next(cudaGraphConditionalHandle h, long long* left) {
   cudaGraphSetConditional(h, v > 0 ? 1u : 0u);
 }
 
-// The whole rollout of nsteps >= 1 steps from the x-inverse of U as one graph:
+// The whole rollout of nsteps >= 1 steps from the x-inverse of U as one graph
+// (step(fuse_next, stream) enqueues one step):
 //   k_loop_arm -> while (left > 0) { step that ends with the next step's
 //   x-inverse; k_loop_next } -> last step.
 // The loop count lives in device memory (P.loop), so one instantiated graph
 // serves every nsteps: the lax.scan of integrators.py:41-53 without a host
 // launch per step.
-template <typename T>
-int build_rollout_graph(hit_plan* p, Path& P, const Scalars& s, double dt, const V2<T>* fext,
-                        cudaGraphExec_t* exec) {
+template <class STEP>
+int build_loop_graph(hit_plan* p, Path& P, STEP&& step, cudaGraphExec_t* exec) {
   int rc;
   cudaGraph_t g = nullptr;
   HIT_CK(cudaGraphCreate(&g, 0));
@@ -529,7 +630,7 @@ int build_rollout_graph(hit_plan* p, Path& P, const Scalars& s, double dt, const
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   // loop body: one step that prepares the next, then the count
   HIT_CK(cudaStreamBeginCaptureToGraph(p->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  rc = enqueue_step<T>(p, P, s, dt, true, fext, p->cap);
+  rc = step(true, p->cap);
   if (!rc) k_loop_next<<<1, 1, 0, p->cap>>>(h, left);
   cudaGraph_t got = nullptr;
   cudaError_t e = cudaStreamEndCapture(p->cap, &got);
@@ -538,12 +639,20 @@ int build_rollout_graph(hit_plan* p, Path& P, const Scalars& s, double dt, const
   if (e != cudaSuccess) return cuda_fail(e, "rollout loop body capture");
   // after the loop: the last step
   HIT_CK(cudaStreamBeginCaptureToGraph(p->cap, g, &loop, nullptr, 1, cudaStreamCaptureModeThreadLocal));
-  rc = enqueue_step<T>(p, P, s, dt, false, fext, p->cap);
+  rc = step(false, p->cap);
   e = cudaStreamEndCapture(p->cap, &got);
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(e, "rollout last-step capture");
   HIT_CK(cudaGraphInstantiate(exec, g, 0));
   return HIT_OK;
+}
+
+template <typename T>
+int build_rollout_graph(hit_plan* p, Path& P, const Scalars& s, double dt, const V2<T>* fext,
+                        cudaGraphExec_t* exec) {
+  return build_loop_graph(
+      p, P, [&](bool fuse_next, cudaStream_t cs) { return enqueue_step<T>(p, P, s, dt, fuse_next, fext, cs); },
+      exec);
 }
 
 template <typename T>
@@ -581,6 +690,54 @@ int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
     HIT_CK(cudaGraphLaunch(P.exec, st));
   }
   HIT_CK(launch_scatter<T>(vp<T>(P.U), static_cast<V2<T>*>(out), P.g, st));
+  return HIT_OK;
+}
+
+// Coarse-LES rollout with the closure fused into the first stage of every
+// step (float32, dealiased path): gather, the LES x-inverse, the steps as one
+// graph with a device-side loop (or enqueued into the caller's capture),
+// scatter.
+int les_rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, const hit_mlp_weights& w, int* err,
+                     double dt, int64_t nsteps, void* out, cudaStream_t st) {
+  int rc;
+  if ((rc = ensure_path<float>(p, 1))) return rc;
+  Path& P = p->path[1];
+  const Scalars s = scalars_of(pr);
+  const Geom& g = P.g;
+  const size_t V = sizeof(float2);
+  if ((rc = ensure(P.t12, (size_t)12 * g.Nx * g.My * g.Mzp * V))) return rc;
+  if ((rc = ensure(P.u12, (size_t)12 * g.Nx * g.Ny * g.Mzp * V))) return rc;
+  if ((rc = ensure(P.FEXT, (size_t)3 * g.Mx * g.My * g.Mzp * V))) return rc;
+  if ((rc = ensure(P.loop, sizeof(long long)))) return rc;
+  if ((rc = gather_state<float>(p, P, u_hat, s, st))) return rc;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HIT_CK(cudaStreamIsCapturing(st, &cs));
+  if (nsteps > 0 && cs != cudaStreamCaptureStatusNone) {
+    if ((rc = launch_p1_of<float>(p, P, vp<float>(P.U), st, true))) return rc;
+    for (int64_t i = 0; i < nsteps; ++i)
+      if ((rc = enqueue_les_step(p, P, s, dt, i + 1 < nsteps, w, err, st))) return rc;
+  } else if (nsteps > 0) {
+    const GraphKey key{s.nu, s.A, s.eps, pr->kmin, pr->kmax, s.E_target, s.tau, dt, s.forcing, s.ifrk, 2};
+    const bool same_w = std::memcmp(&P.les_w, &w, sizeof(w)) == 0 && P.les_err == err;
+    if (!P.les_key_valid || !(P.les_key == key) || !same_w) {
+      if (P.les_exec) cudaGraphExecDestroy(P.les_exec);
+      P.les_exec = nullptr;
+      P.les_key_valid = false;
+      if ((rc = build_loop_graph(
+               p, P, [&](bool fuse_next, cudaStream_t c) { return enqueue_les_step(p, P, s, dt, fuse_next, w, err, c); },
+               &P.les_exec)))
+        return rc;
+      P.les_key = key;
+      P.les_w = w;
+      P.les_err = err;
+      P.les_key_valid = true;
+    }
+    k_loop_set<<<1, 1, 0, st>>>(static_cast<long long*>(P.loop.p), (long long)(nsteps - 1));
+    HIT_CK(cudaGetLastError());
+    if ((rc = launch_p1_of<float>(p, P, vp<float>(P.U), st, true))) return rc;
+    HIT_CK(cudaGraphLaunch(P.les_exec, st));
+  }
+  HIT_CK(launch_scatter<float>(vp<float>(P.U), static_cast<float2*>(out), P.g, st));
   return HIT_OK;
 }
 
@@ -1101,7 +1258,10 @@ int hit_plan_destroy(hit_plan* p) {
   DeviceGuard dg(p->device);
   for (Path& P : p->path) {
     if (P.exec) cudaGraphExecDestroy(P.exec);
+    if (P.les_exec) cudaGraphExecDestroy(P.les_exec);
     release(P.loop);
+    release(P.t12);
+    release(P.u12);
     release(P.t6);
     release(P.u6);
     release(P.U);
@@ -1234,6 +1394,24 @@ int hit_rk4_step(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
   if ((rc = check_params(pr))) return rc;
   DeviceGuard dg(p->device);
   return DISPATCH(p, rollout_impl)(p, u_hat, pr, dt, 1, out, nullptr, (cudaStream_t)stream);
+}
+
+int hit_les_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, const hit_mlp_weights* w, double dt,
+                    int64_t nsteps, void* out, int* err_dev, void* stream) {
+  if (!p || !u_hat || !pr || !w || !out || !err_dev) return fail(HIT_E_INVALID, "NULL argument");
+  if (!w->w1t || !w->w2t || !w->w3t || !w->w4t || !w->b2 || !w->b3 || !w->b4)
+    return fail(HIT_E_INVALID, "les_rollout: NULL MLP weight");
+  if (nsteps < 0) return fail(HIT_E_INVALID, "nsteps must be >= 0");
+  int rc;
+  if ((rc = check_params(pr))) return rc;
+  if (p->dtype != HIT_DTYPE_F32) return fail(HIT_E_UNSUPPORTED, "les_rollout: float32 plans only");
+  if (!(pr->flags & HIT_FLAG_ASSUME_DEALIASED))
+    return fail(HIT_E_UNSUPPORTED, "les_rollout: the state must be dealiased (HIT_FLAG_ASSUME_DEALIASED)");
+  if (pr->flags & HIT_FLAG_INTEGRATING_FACTOR) return fail(HIT_E_UNSUPPORTED, "les_rollout: RK4 only");
+  if (p->Nx > 256 || !zles_supported(p->Nz))
+    return fail(HIT_E_UNSUPPORTED, "les_rollout: needs Nx <= 256 and Nz in {32, 64, 128}");
+  DeviceGuard dg(p->device);
+  return les_rollout_impl(p, u_hat, pr, *w, err_dev, dt, nsteps, out, (cudaStream_t)stream);
 }
 
 int hit_rollout(hit_plan* p, const void* u_hat, const hit_params* pr, double dt, int64_t nsteps, double t0, void* out,

@@ -27,10 +27,10 @@ import time
 import torch
 
 from . import _native as nat
-from .closure import ClosureMLP
+from .closure import ClosureMLP, ctypes_ref
 from .diagnostics import energy, energy_budget, energy_spectrum
 from .fields import cfl_dt, hit_initial_field
-from .forcing import HoldEnergyForcing, LinearForcing
+from .forcing import HoldEnergyForcing, LinearForcing, native_params
 from .grid import _check_state, make_grid, to_physical, to_spectral
 from .integrators import rk4_step, rollout
 from .navierstokes import NSParams, make_ns_rhs
@@ -131,10 +131,21 @@ class FusedLESStep:
     order in dt like the freeze itself), and at small grids, where the step
     kernels leave most SMs idle, the closure's cost is hidden.  All buffers are
     allocated at construction, so a call can be captured into a CUDA graph
-    after one warm-up call."""
+    after one warm-up call.
 
-    def __init__(self, grid, closure, params, dt, lag=False, mlp_ctas_per_sm=1):
+    ``fused=True`` (unlagged, float32, Nz in {32, 64, 128}): the closure runs
+    inside the step's own passes (`hit_les_rollout`): the first stage's
+    x-inverse also emits the nine velocity gradients, its z pass evaluates the
+    MLP per grid point on the tensor cores beside u x w, and its x-forward
+    epilogue adds the force and holds it over the remaining stages -- the
+    same scheme as ``fused=False`` without the separate gradient, MLP,
+    transform and force launches."""
+
+    def __init__(self, grid, closure, params, dt, lag=False, mlp_ctas_per_sm=1, fused=False):
         self.grid, self.closure, self.params, self.dt, self.lag = grid, closure, params, float(dt), bool(lag)
+        self.fused = bool(fused) and closure is not None
+        if self.fused and self.lag:
+            raise ValueError("the fused closure evaluates the force inside the step: no lag")
         # with the lag the MLP shares the GPU with the step: a lighter footprint
         # (fewer CTAs per SM) keeps the step's kernels from waiting for SM space
         self.mlp_ctas_per_sm = int(mlp_ctas_per_sm) if self.lag else 0
@@ -176,6 +187,15 @@ class FusedLESStep:
         u_hat = _check_state(u_hat, self.grid)
         if self.closure is None:
             return rk4_step(self.ns, u_hat, self.params, self.dt, 0.0, assume_dealiased=True, out=out)
+        if self.fused:
+            g = self.grid
+            if getattr(self.closure, "_physical", None) is None:
+                self.closure.pack_physical()
+            p = native_params(self.params.nu, self.params.forcing, nat.HIT_FLAG_ASSUME_DEALIASED)
+            out = torch.empty_like(u_hat) if out is None else out
+            nat.call("hit_les_rollout", g.plan.handle, nat.ptr(u_hat), p, ctypes_ref(self.closure._physical[0]),
+                     self.dt, 1, nat.ptr(out), nat.ptr(self.closure._err), nat.stream_ptr(g.device))
+            return out
         if not self.lag:
             f = self.force(u_hat)
             return rk4_step(self.ns, u_hat, self.params, self.dt, 0.0, assume_dealiased=True, f_ext=f, out=out)
@@ -320,12 +340,13 @@ def train(data, steps=400, batch_snapshots=16, lr=2e-3, seed=0, val_snapshots=20
 
 
 def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True, tau_relax=0.5, freeze_every=4,
-            fused=True, lag=False, forcing=None):
+            fused=True, lag=False, forcing=None, fused_closure=False):
     """Coarse LES from the first filtered snapshot's state with the DNS's
     Lundgren forcing holding the total energy of the filtered DNS field (its
     mean over the snapshots; relaxation time ``tau_relax``), the SGS stress
     evaluated once per RK4 step (``freeze_every`` = 4; `FusedLESStep` when
-    ``fused``, else the composed `LESRHS` step; ``lag``: the fused step's
+    ``fused``, else the composed `LESRHS` step; ``fused_closure``: the closure
+    inside the step's passes, see `FusedLESStep`; ``lag``: the fused step's
     lagged closure; ``forcing`` replaces the hold-energy forcing); returns the time-averaged
     spectrum over the samples after ``discard`` steps, the step time and the
     energy history."""
@@ -336,7 +357,7 @@ def run_les(data, closure, steps=5000, sample_every=50, discard=1000, graph=True
     u = data["u0_coarse"].clone()
     dt = data.get("dt_les") or cfl_dt(u, coarse, 0.5)
     if fused and freeze_every == 4:
-        step = FusedLESStep(coarse, closure, p, dt, lag=lag)
+        step = FusedLESStep(coarse, closure, p, dt, lag=lag, fused=fused_closure)
     else:
         rhs = LESRHS(coarse, closure, freeze_every=freeze_every)
 

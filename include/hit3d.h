@@ -262,6 +262,23 @@ int hit_add_sgs_force(hit_plan *plan, const void *tau_hat, void *du_hat,
 int hit_sgs_force(hit_plan *plan, const void *tau_hat, void *f_hat,
                   void *stream);
 
+/* Coarse-LES rollout with the closure fused into the solver's passes (no
+ * reference counterpart; the step it replaces is the reference RHS,
+ * src/hit3d/navierstokes.py:69-95, plus the SGS force).  Every RK4 step
+ * evaluates the closure at its initial state inside its first stage: the
+ * x-inverse also emits the nine velocity gradients, the z pass forms w from
+ * them, u x w and the MLP's six stresses per grid point (w: the same weights
+ * as hit_mlp_forward_strided, inputs the gradients in physical units), and
+ * the x-forward epilogue adds f = project(dealias(-1j k_j tau_hat_ij)) and
+ * holds it over stages 2-4 (the scheme of hit_velocity_gradients +
+ * hit_mlp_forward_strided + rfftn + hit_sgs_force + hit_rollout_forced with
+ * nsteps = 1).  float32 plans, HIT_FLAG_ASSUME_DEALIASED, RK4, Nx <= 256 and
+ * Nz in {32, 64, 128}; *err_dev is set when an MMA wait gave up.  Same
+ * capture and graph behaviour as hit_rollout. */
+int hit_les_rollout(hit_plan *plan, const void *u_hat, const hit_params *params,
+                    const hit_mlp_weights *w, double dt, int64_t nsteps,
+                    void *out, int *err_dev, void *stream);
+
 /* Bytes of DEVICE workspace hit_mlp_train_grads needs for P points. */
 int64_t hit_mlp_workspace_bytes(int64_t P);
 
