@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(NTZ, MINB) k_zcross(ZCrossArgs<T> a) {
 constexpr int ZLES_MMA_WAIT = 1 << 22;  // mbarrier polls before an MMA wait gives up
 
 template <int H>
-__global__ void __launch_bounds__(128) k_zles(ZLesArgs a) {
+__global__ void __launch_bounds__(128, 4) k_zles(ZLesArgs a) {
   constexpr int NZ = 2 * H, RB = 128 / NZ, NTZ = 128;
   using AD = SkewAddr<skew_ld(H)>;
   constexpr int RS = z_row_cap<H>();
@@ -748,9 +748,9 @@ template <int HH> cudaError_t launch_zles_v(const ZLesArgs& a, cudaStream_t st) 
                                 cudaSharedmemCarveoutMaxShared);
   });
   if (e != cudaSuccess) return e;
-  // resident CTAs from the SM's shared memory (the occupancy query counts one
-  // CTA per SM for kernels that allocate tensor memory), at most 8 per SM (8 x
-  // 64 TMEM columns)
+  // resident CTAs from the SM's shared memory and registers (the occupancy
+  // query counts one CTA per SM for kernels that allocate tensor memory), at
+  // most 8 per SM (8 x 64 TMEM columns)
   std::atomic<int>* slot = cache.here();
   int wave = slot ? slot->load(std::memory_order_relaxed) : 0;
   if (wave == 0) {
@@ -759,7 +759,12 @@ template <int HH> cudaError_t launch_zles_v(const ZLesArgs& a, cudaStream_t st) 
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
       return e;
-    const int per_sm = std::max(1, std::min((int)(smem_sm / (smem + 1024 + 64)), 8));
+    int regs_sm = 0;
+    cudaFuncAttributes fa{};
+    if ((e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, k_zles<HH>)) != cudaSuccess) return e;
+    const int by_regs = regs_sm / (128 * ((std::max(fa.numRegs, 1) + 7) / 8 * 8));
+    const int per_sm = std::max(1, std::min(std::min((int)(smem_sm / (smem + 1024 + 64)), by_regs), 8));
     wave = per_sm * std::max(sms, 1);
     if (slot) slot->store(wave, std::memory_order_relaxed);
   }

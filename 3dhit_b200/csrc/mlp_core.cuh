@@ -117,13 +117,21 @@ __device__ __forceinline__ void infer_tile(InferSmem& S, const float (&x9)[9], f
     phase ^= 1;
     tc::fence_after_sync();
   };
-  auto ld64 = [&](float (&v)[64]) {
+  // the 64 accumulator columns of this thread's point, 16 at a time: plus
+  // the bias, GELU, rounded to bf16 into the next layer's input tile (a live
+  // set of 16 values instead of 64)
+  auto act64 = [&](const float* bias) {
 #pragma unroll
     for (int c = 0; c < 64; c += 16) {
       float t[16];
       tc::tmem_ld16(lane_base + c, t);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) v[c + i] = t[i];
+      for (int h = 0; h < 2; ++h) {
+        __align__(16) __nv_bfloat16 q[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) q[i] = __float2bfloat16_rn(gelu(t[8 * h + i] + (bias ? bias[c + 8 * h + i] : 0.f)));
+        *reinterpret_cast<uint4*>(S.buf + tc::kmajor_off(tid, c + 8 * h, 64)) = *reinterpret_cast<const uint4*>(q);
+      }
     }
   };
   {
@@ -133,22 +141,14 @@ __device__ __forceinline__ void infer_tile(InferSmem& S, const float (&x9)[9], f
     x[15] = 1.f;  // bias input of layer 1
     store_row<16>(S.x0, tid, x, 16);
   }
-  float v[64];
+  // (a layer's input tile is rewritten only after the MMA that reads it has
+  // completed: mma() returns after its completion wait)
   mma(S.x0, 16, S.w1t, 16, 1, id64);
-  ld64(v);
-#pragma unroll
-  for (int i = 0; i < 64; ++i) v[i] = gelu(v[i]);
-  store_row<64>(S.buf, tid, v, 64);
+  act64(nullptr);
   mma(S.buf, 64, S.w2t, 64, 4, id64);
-  ld64(v);
-#pragma unroll
-  for (int i = 0; i < 64; ++i) v[i] = gelu(v[i] + S.b2[i]);
-  store_row<64>(S.buf, tid, v, 64);
+  act64(S.b2);
   mma(S.buf, 64, S.w3t, 64, 4, id64);
-  ld64(v);
-#pragma unroll
-  for (int i = 0; i < 64; ++i) v[i] = gelu(v[i] + S.b3[i]);
-  store_row<64>(S.buf, tid, v, 64);
+  act64(S.b3);
   mma(S.buf, 64, S.w4t, 64, 4, id16);
   float y[16];
   tc::tmem_ld16(lane_base, y);

@@ -560,8 +560,9 @@ def run_closure(args):
     kc = data["coarse"].Nx // 3
     out = {}
 
-    def les_record(name, cl, lag):
-        r = les.run_les(data, cl, steps=args.cl_les_steps, discard=args.cl_les_steps // 5, lag=lag)
+    def les_record(name, cl, lag, fused=False):
+        r = les.run_les(data, cl, steps=args.cl_les_steps, discard=args.cl_les_steps // 5, lag=lag,
+                        fused_closure=fused)
         rel = (r["spectrum"] / ref - 1).abs()
         T = args.cl_les_steps * r["dt"]
         dns_wall = T / data["dt"] * data["dns_ms_per_step"]
@@ -585,6 +586,8 @@ def run_closure(args):
     t_apost = time.perf_counter() - t1
     les_record("closure_a_posteriori", model, False)
     les_record("closure_a_posteriori_lagged", model, True)
+    # the closure inside the step's own passes (hit_les_rollout)
+    les_record("closure_a_posteriori_fused", model, False, True)
     line = {"metric": f"closure-LES {args.cl_coarse}^3 vs filtered {args.cl_fine}^3 DNS: max E(k) rel err, k<=k_c",
             "value": out["closure_a_posteriori"]["max_rel_err_Ek"], "unit": "fraction", "higher_is_better": False,
             "fallback_value": out["no_closure"]["max_rel_err_Ek"],
