@@ -155,6 +155,10 @@ struct hit_plan {
   // cotangents, and the rollout checkpoints
   Buf ax9, aph, as6, apart, asums, ascal, apct, ast[3], ak, akb, asb, aacc, aub, ack, aseg, afb;
   cudaStream_t cap = nullptr;  // private stream used only for graph capture
+  // side branch of the step for the forcing coefficient's reduction (see
+  // fork_coef): its stream and one fork / join event pair per RK4 stage
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork[4] = {}, ev_join[4] = {};
 };
 
 namespace {
@@ -469,16 +473,41 @@ int launch_p3_stage(hit_plan* p, Path& P, const Scalars& s, int stage, double dt
 // (left by the previous step's last stage or by a standalone k_p1).  With
 // fuse_next the last stage also runs the x-inverse of the new state for the
 // following step.
+// The forcing coefficient of the next stage input, reduced on a side branch
+// of the step: fork after the k_p3 that wrote its partial sums, join just
+// before the k_p3 that reads it, so that the one-block reduction runs beside
+// the next stage's y-inverse, z pass and y-forward instead of between them
+// (in a captured graph: a parallel branch with its own edges).
+template <typename T> int fork_coef(hit_plan* p, Path& P, const Scalars& s, int k, cudaStream_t st) {
+  HIT_CK(cudaEventRecord(p->ev_fork[k], st));
+  HIT_CK(cudaStreamWaitEvent(p->side, p->ev_fork[k], 0));
+  int rc;
+  if ((rc = launch_coef<T>(p, P, s, P.p3_blocks, p->side))) return rc;
+  HIT_CK(cudaEventRecord(p->ev_join[k], p->side));
+  return HIT_OK;
+}
+int join_coef(hit_plan* p, int k, cudaStream_t st) {
+  HIT_CK(cudaStreamWaitEvent(st, p->ev_join[k], 0));
+  return HIT_OK;
+}
+
 template <typename T>
 int enqueue_step(hit_plan* p, Path& P, const Scalars& s, double dt, bool fuse_next, const V2<T>* fext,
                  cudaStream_t st, Prof* pf = nullptr) {
   int rc;
   const bool red = needs_coef(s.forcing);
+  const bool branch = red && !pf;  // timed runs keep every kernel on the one stream
   for (int stage = 1; stage <= 4; ++stage) {
     if ((rc = launch_p2<T>(p, P, st, pf))) return rc;
+    if (branch && stage > 1 && (rc = join_coef(p, stage - 2, st))) return rc;
     TIMED(pf, 4, launch_p3_stage<T>(p, P, s, stage, dt, stage < 4 || fuse_next, red, fext, st));
-    if (red) TIMED(pf, 5, launch_coef<T>(p, P, s, P.p3_blocks, st));
+    if (branch) {
+      if ((rc = fork_coef<T>(p, P, s, stage - 1, st))) return rc;
+    } else if (red) {
+      TIMED(pf, 5, launch_coef<T>(p, P, s, P.p3_blocks, st));
+    }
   }
+  if (branch && (rc = join_coef(p, 3, st))) return rc;  // the next step's first stage reads it
   return HIT_OK;
 }
 
@@ -500,12 +529,14 @@ int enqueue_les_step(hit_plan* p, Path& P, const Scalars& s, double dt, bool fus
       if ((rc = launch_p3_stage<float>(p, P, s, 1, dt, true, red, nullptr, st, true, false))) return rc;
     } else {
       if ((rc = launch_p2<float>(p, P, st))) return rc;
+      if (red && (rc = join_coef(p, stage - 2, st))) return rc;
       if ((rc = launch_p3_stage<float>(p, P, s, stage, dt, stage < 4 || fuse_next, red, f, st, false,
                                        stage == 4 && fuse_next)))
         return rc;
     }
-    if (red && (rc = launch_coef<float>(p, P, s, P.p3_blocks, st))) return rc;
+    if (red && (rc = fork_coef<float>(p, P, s, stage - 1, st))) return rc;
   }
+  if (red && (rc = join_coef(p, 3, st))) return rc;
   return HIT_OK;
 }
 
@@ -1243,7 +1274,12 @@ int hit_plan_create(int nx, int ny, int nz, double lx, double ly, double lz, int
   int rc = dtype == HIT_DTYPE_F32 ? create_impl<float>(p) : create_impl<double>(p);
   if (rc == HIT_OK) {
     e = cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking);
-    if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreate");
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+      e = cudaEventCreateWithFlags(&p->ev_fork[k], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_join[k], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreate / cudaEventCreate");
   }
   if (rc != HIT_OK) {
     hit_plan_destroy(p);
@@ -1280,6 +1316,11 @@ int hit_plan_destroy(hit_plan* p) {
                  &p->ast[2], &p->ak, &p->akb, &p->asb, &p->aacc, &p->aub, &p->ack, &p->aseg, &p->afb})
     release(*b);
   if (p->cap) cudaStreamDestroy(p->cap);
+  if (p->side) cudaStreamDestroy(p->side);
+  for (int k = 0; k < 4; ++k) {
+    if (p->ev_fork[k]) cudaEventDestroy(p->ev_fork[k]);
+    if (p->ev_join[k]) cudaEventDestroy(p->ev_join[k]);
+  }
   delete p;
   return HIT_OK;
 }
