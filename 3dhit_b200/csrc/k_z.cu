@@ -422,6 +422,12 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
       }
     }
     float2 u0[8], u1[8], u2[8], n0[8], n1[8], n2[8];
+    // e^{-2 pi i k / Nz} of this lane's positions k = b + (H/8) r, loaded once
+    // for the pre-processing of the six fields and the post-processing of the
+    // three products
+    float2 wz[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) wz[r] = twz[b + Z::NB0 * r];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       // c2r pre-processing of positions k = b + (H/8) r (see c2r_pre)
@@ -438,7 +444,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
         }
         Y.y = -Y.y;
         const float2 sm = cadd(X, Y), df = csub(X, Y);
-        float2 w = twz[k];
+        float2 w = wz[r];
         w.y = -w.y;
         v[r] = cadd(sm, cmul_i(cmul(w, df)));
       }
@@ -493,7 +499,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
             float2 bc = zb;
             bc.y = -bc.y;
             const float2 E = cadd(v[r], bc), O = cmul_mi(csub(v[r], bc));
-            x = cadd(E, cmul(twz[k], O));
+            x = cadd(E, cmul(wz[r], O));
           }
           out[k] = x;
         }
