@@ -857,11 +857,19 @@ __device__ __forceinline__ void p1m_body(float2* A, float2* B, int j, int z0, co
   });
 }
 
-// One (ky row, z tile) of k_p3m.  stg holds the staged first nl component.
+// State-array tensor maps of k_p3m's epilogue ring (see p3m_state_map): the
+// stage input (u for stages 0/1, s after), the accumulator and u.
+struct P3mMaps {
+  CUtensorMap us, acc, u;
+};
+
+// One (ky row, z tile) of k_p3m.  stg holds the staged first nl component;
+// the ring slots' mbarriers are mb0 and mb0 + 8, and bit k of ph is slot k's
+// phase.  False when a ring wait gave up (the CTA then stops).
 template <int N, int W>
-__device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, float2* B, const float2* tws,
+__device__ __forceinline__ bool p3m_tile(const P3Args<float>& a, float2* A, float2* B, const float2* tws,
                                          double* red, int j, int z0, int tile, float2* stg, int nzt, int ntiles,
-                                         uint32_t tm) {
+                                         uint32_t tm, const P3mMaps& maps, uint32_t mb0, uint32_t& ph) {
   constexpr int NTH = P3M_THREADS, NB = N / 8;
   const Geom& g = a.g;
   constexpr int CPR = W / 2;  // 16-byte chunks per row
@@ -904,9 +912,13 @@ __device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, floa
 
   // epilogue: pass r covers positions r N/8 .. r N/8 + N/8 - 1 (b_i + r N/8 of
   // every thread); passes whose positions are all outside the stored rows are
-  // skipped.  The state rows of a pass are staged into A or B (a 2-slot ring)
-  // with cp.async, the next pass's while this one is computed.
-  const float2* __restrict__ us_arr = a.stage <= 1 ? a.u : a.s;
+  // skipped.  The state rows of a pass are staged into A or B (a 2-slot ring),
+  // the next pass's while this one is computed: one thread issues one TMA box
+  // per state array (W columns x 1 ky row x N/8 compact rows x 3 components),
+  // counted in bytes on the slot's mbarrier.  The box starts at the compact
+  // row of the pass's first position in the half it begins in; rows of a box
+  // that fall in the 2/3-rule gap or past the array land at positions that are
+  // not stored (never read) or are zero-filled by the TMA unit.
   auto stored = [&](int r) {  // does pass r hold a stored row (uniform)
     return r * NB < g.hx || (r + 1) * NB > g.hx + (N - g.Mx);
   };
@@ -914,18 +926,20 @@ __device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, floa
     while (r < 8 && !stored(r)) ++r;
     return r;
   };
-  auto stage_pass = [&](int r, float2* slot) {
-    if (r < 8) {
-      for (int e = threadIdx.x; e < nq * NB * CPR; e += NTH) {
-        const int q = e / (NB * CPR), rem = e % (NB * CPR), lr = rem / CPR, ch = rem % CPR;
-        const int i = compact_row(r * NB + lr, g.hx, g.Mx, N);
-        if (i >= 0) {
-          const float2* arr = q < 3 ? us_arr : (q < 6 ? a.acc : a.u);
-          cp_async16(slot + (q * NB + lr) * W + ch * 2, arr + (q % 3) * a.c_c + cbase + (long long)i * a.c_x + ch * 2);
-        }
+  const int narr = a.stage <= 1 ? 1 : 3;
+  auto stage_pass = [&](int r, int k) {  // pass r into slot k (no-op for r = 8)
+    if (r < 8 && threadIdx.x == 0) {
+      float2* slot = k ? B : A;
+      const int x0 = r * NB < g.hx ? r * NB : r * NB - (N - g.Mx);
+      tma::fence_async_smem();  // the slot's earlier generic accesses come first
+      const uint32_t mbk = mb0 + 8u * k;
+      tma::mbar_expect_tx(mbk, (uint32_t)(narr * 3 * NB * W * sizeof(float2)));
+      tma::load4(slot, &maps.us, z0, j, x0, 0, mbk);
+      if (narr == 3) {
+        tma::load4(slot + 3 * NB * W, &maps.acc, z0, j, x0, 0, mbk);
+        tma::load4(slot + 6 * NB * W, &maps.u, z0, j, x0, 0, mbk);
       }
     }
-    cp_async_commit();
   };
   const int fy = full_pos(j, g.hy, g.My, g.Ny);
   const float ky = a.k.ky[fy];
@@ -938,8 +952,8 @@ __device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, floa
   __syncthreads();  // every thread has left the last forward stage: A and B are free
   int rc = next_pass(0);
   int rn = next_pass(rc + 1);
-  stage_pass(rc, A);
-  stage_pass(rn, B);
+  stage_pass(rc, 0);
+  stage_pass(rn, 1);
   const float zeros[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   int k = 0;
 #pragma unroll 1
@@ -949,9 +963,21 @@ __device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, floa
       tc::tmem_st2x3(tm + 16 + 2 * r, 32, zeros);
       continue;
     }
-    float2* slot = (k & 1) ? B : A;
-    cp_async_wait_group<1>();
-    __syncthreads();
+    const int sk = k & 1;
+    float2* slot = sk ? B : A;
+    {
+      // the pass's boxes have landed (a verdict shared by the block)
+      const uint32_t mbk = mb0 + 8u * sk, par = (ph >> sk) & 1u;
+      const bool ok = __syncthreads_and(tma::mbar_wait(mbk, par, g_axis_wait_limit)) != 0;
+      ph ^= 1u << sk;
+      if (!ok) {
+        if (threadIdx.x == 0) atomicExch(&g_axis_timeout, 1);
+        tma::mbar_wait(mbk, par, AXIS_WAIT);  // the copies in flight, once more with a limit
+        if (rn < 8) tma::mbar_wait(mb0 + 8u * (sk ^ 1), (ph >> (sk ^ 1)) & 1u, AXIS_WAIT);
+        tc::tmem_wait_st();
+        return false;
+      }
+    }
     float d[12];
     tc::tmem_ld2x3x2(tm + 2 * r, 32, 16, d);  // [6 i + 2 c]: component c of butterfly i
 #pragma unroll
@@ -981,7 +1007,7 @@ __device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, floa
     }
     __syncthreads();  // the slot is read: it takes the pass after next
     const int r2 = next_pass(rn + 1);
-    stage_pass(r2, slot);
+    stage_pass(r2, sk);
     rc = rn;
     rn = r2;
     ++k;
@@ -996,25 +1022,38 @@ __device__ __forceinline__ void p3m_tile(const P3Args<float>& a, float2* A, floa
     }
   }
   if (a.fuse_p1) p1m_body<N, W>(A, B, j, z0, g, a.k, tws, a.t6, a.t6_c, a.t6_x, tm);
+  return true;
 }
 
 template <int N, int W>
-__global__ void __launch_bounds__(P3M_THREADS, 2) k_p3m(P3Args<float> a, int nzt, int ntiles) {
+__global__ void __launch_bounds__(P3M_THREADS, 2) k_p3m(P3Args<float> a, int nzt, int ntiles,
+                                                       const __grid_constant__ P3mMaps maps) {
   static_assert(p3m_fits<N, W>(), "two radix-8 butterflies per thread at the first and last stage");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ double red[96];
   __shared__ uint32_t tslot;
-  float2* A = reinterpret_cast<float2*>(smem_raw);
+  __shared__ __align__(8) uint64_t rbar[2];
+  // the ring's TMA boxes land in A and B: 128-byte aligned by hand (the
+  // dynamic shared memory follows the static variables with 16-byte alignment
+  // only; p3m_smem reserves the 128 bytes)
+  float2* A = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
   float2* B = A + skew8_slots(N, W);
   float2* stg = B + skew8_slots(N, W);  // staged N x W column of the next nl component
   float2* tws = stg + N * W;
   fill_stage_twiddles<float, N, false, P3M_THREADS>(tws, a.tw);
   const int warp = threadIdx.x >> 5;
   if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tslot), P3M_COLS);
+  const uint32_t mb0 = tma::smem_u32(&rbar[0]);  // rbar[1] at mb0 + 8
+  if (threadIdx.x == 0) {
+    tma::mbar_init(mb0, 1);
+    tma::mbar_init(mb0 + 8, 1);
+  }
+  tma::fence_async_smem();
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tm = tslot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(warp >> 2) * 128;
+  uint32_t ph = 0;
   pdl_wait();
   pdl_trigger();
   if (blockIdx.x < ntiles) {
@@ -1029,7 +1068,7 @@ __global__ void __launch_bounds__(P3M_THREADS, 2) k_p3m(P3Args<float> a, int nzt
   }
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int j = tile / nzt, z0 = (tile % nzt) * W;
-    p3m_tile<N, W>(a, A, B, tws, red, j, z0, tile, stg, nzt, ntiles, tm);
+    if (!p3m_tile<N, W>(a, A, B, tws, red, j, z0, tile, stg, nzt, ntiles, tm, maps, mb0, ph)) break;
   }
   cp_async_wait_all();
   tc::fence_before_sync();
@@ -1229,9 +1268,28 @@ template <typename T, int NN, int W, int NTH> cudaError_t launch_p3_v(const P3Ar
                     NTH, smem, st, a, nzt, ntiles);
 }
 
-// k_p3m shared memory: A, B, the staged nl column (N x W) and the twiddles.
+// k_p3m shared memory: A, B, the staged nl column (N x W) and the twiddles,
+// plus 128 bytes for aligning A.
 template <int N, int W> constexpr size_t p3m_smem() {
-  return sizeof(float2) * ((size_t)2 * skew8_slots(N, W) + N * W + tw_slots_even<N>());
+  return sizeof(float2) * ((size_t)2 * skew8_slots(N, W) + N * W + tw_slots_even<N>()) + 128;
+}
+
+// Tensor map of k_p3m's epilogue ring over a compact state array (3, Mx, My,
+// Mzp) of complex values: dims (z, ky row, compact x row, component) in
+// 8-byte elements, box (W, 1, rows, 3); the boxes start at multiples of W in
+// z (64-byte aligned), the other coordinates may run past the array (zero
+// fill).
+bool p3m_state_map(CUtensorMap* m, const float2* base, const Geom& g, long long c_x, long long c_c, int W, int rows) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc || ((uintptr_t)base % 16) || g.Mzp % 2) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)g.Mzp, (cuuint64_t)g.My, (cuuint64_t)g.Mx, 3};
+  const cuuint64_t strides[3] = {(cuuint64_t)g.Mzp * sizeof(float2), (cuuint64_t)c_x * sizeof(float2),
+                                 (cuuint64_t)c_c * sizeof(float2)};
+  const cuuint32_t box[4] = {(cuuint32_t)W, 1, (cuuint32_t)rows, 3};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, const_cast<float2*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int NN, int W> cudaError_t launch_p3m_v(const P3Args<float>& a, cudaStream_t st) {
@@ -1239,6 +1297,12 @@ template <int NN, int W> cudaError_t launch_p3m_v(const P3Args<float>& a, cudaSt
   cudaError_t e = once_per_device(ready, [] { return max_smem(k_p3m<NN, W>, (int)p3m_smem<NN, W>()); });
   if (e != cudaSuccess) return e;
   const int nzt = a.g.Mzp / W, ntiles = nzt * a.g.My;
+  P3mMaps maps{};
+  constexpr int NB = NN / 8;
+  if (!p3m_state_map(&maps.us, a.stage <= 1 ? a.u : a.s, a.g, a.c_x, a.c_c, W, NB) ||
+      !p3m_state_map(&maps.acc, a.acc, a.g, a.c_x, a.c_c, W, NB) ||
+      !p3m_state_map(&maps.u, a.u, a.g, a.c_x, a.c_c, W, NB))
+    return cudaErrorInvalidValue;
   // Resident CTAs: the occupancy query counts one CTA per SM for kernels that
   // allocate tensor memory, so the wave is sized from the SM's shared memory
   // and registers, at most 2 per SM (two 256-column TMEM allocations fill it).
@@ -1259,7 +1323,7 @@ template <int NN, int W> cudaError_t launch_p3m_v(const P3Args<float>& a, cudaSt
     if (slot) slot->store(wave, std::memory_order_relaxed);
   }
   return launch_pdl(k_p3m<NN, W>, ntiles < wave ? std::max(ntiles, 1) : wave, P3M_THREADS, p3m_smem<NN, W>(), st, a,
-                    nzt, ntiles);
+                    nzt, ntiles, maps);
 }
 
 // Threads per k_p1/k_p3 CTA: 512 (one CTA per SM at 512- and 1024-point

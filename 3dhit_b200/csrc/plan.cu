@@ -698,9 +698,10 @@ int rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, double dt
   if ((rc = gather_state<T>(p, P, u_hat, s, st))) return rc;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   HIT_CK(cudaStreamIsCapturing(st, &cs));
-  if (nsteps > 0 && cs != cudaStreamCaptureStatusNone) {
-    // the caller is capturing `st` into its own graph: enqueue the step
-    // kernels themselves instead of launching the plan's step graphs
+  if (nsteps == 1 || (nsteps > 0 && cs != cudaStreamCaptureStatusNone)) {
+    // the caller is capturing `st` into its own graph, or a single step (a
+    // graph with a conditional node would hide its kernels from per-kernel
+    // profilers): enqueue the step kernels themselves
     if ((rc = launch_p1_of<T>(p, P, vp<T>(P.U), st))) return rc;
     for (int64_t i = 0; i < nsteps; ++i)
       if ((rc = enqueue_step<T>(p, P, s, dt, i + 1 < nsteps, fext ? vp<T>(P.FEXT) : nullptr, st))) return rc;
@@ -743,7 +744,7 @@ int les_rollout_impl(hit_plan* p, const void* u_hat, const hit_params* pr, const
   if ((rc = gather_state<float>(p, P, u_hat, s, st))) return rc;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   HIT_CK(cudaStreamIsCapturing(st, &cs));
-  if (nsteps > 0 && cs != cudaStreamCaptureStatusNone) {
+  if (nsteps == 1 || (nsteps > 0 && cs != cudaStreamCaptureStatusNone)) {
     if ((rc = launch_p1_of<float>(p, P, vp<float>(P.U), st, true))) return rc;
     for (int64_t i = 0; i < nsteps; ++i)
       if ((rc = enqueue_les_step(p, P, s, dt, i + 1 < nsteps, w, err, st))) return rc;

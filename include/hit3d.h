@@ -150,8 +150,8 @@ int hit_rk4_step(hit_plan *plan, const void *u_hat, const hit_params *params,
 
 /* rollout (src/hit3d/integrators.py:41-53): nsteps RK4 steps as one launch of
  * a CUDA graph that loops over the steps on the device (a while conditional
- * node counting down a step count in device memory); no host synchronisation
- * inside.  When the stream is
+ * node counting down a step count in device memory; one step is enqueued
+ * directly); no host synchronisation inside.  When the stream is
  * being captured by the caller (cudaStreamIsCapturing), the step kernels are
  * enqueued themselves, so a rollout can be part of the caller's graph (the
  * plan's buffers must exist by then: call once before capturing). */

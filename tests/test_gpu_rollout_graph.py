@@ -1,8 +1,10 @@
 """The rollout as one CUDA graph with a device-side while loop
 (`hit_rollout`, reference `rollout`, src/hit3d/integrators.py:41-53): one
 instantiated graph serves every step count, the loop count living in device
-memory.  Rollouts of 1, 4, 2 and 7 steps on the same plan, one after the
-other, must equal the same number of one-step rollouts (to float32 rounding:
+memory (a single step is enqueued without the graph, whose conditional node
+would hide its kernels from per-kernel profilers).  Rollouts of 1, 4, 2 and
+7 steps on the same plan, one after the other, must equal the same number
+of one-step rollouts (to float32 rounding:
 a one-step rollout starts from the state's own x-inverse and forcing sums,
 a longer one from those its previous step fused; a step too many or too few
 moves the state by ~1e-3), and a 6-step rollout must match the oracle."""
