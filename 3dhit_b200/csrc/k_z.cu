@@ -518,6 +518,178 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
   }
 }
 
+// k_zpair: k_zwarp for rows of Nz = 1024 (H = 512).  A row's half-length
+// transform needs 64 lanes of 8 values, so a team of two warps owns each row,
+// and its exchanges are ordered by a named barrier over the team's 64 threads
+// (barrier 1 + team; 0 is __syncthreads).  The r2c post-processing partner
+// Z[H - k] of lane b is lane (64 - b) mod 64, in the other warp for most b:
+// the transform's outputs go through the exchange buffer instead of a
+// shuffle.  Staging (one bulk TMA copy per input row, issued by the team's
+// first warp on the team's mbarrier), pre-processing, u x w in registers and
+// the outputs over the first three input rows are k_zwarp's.  A give-up of the
+// staging wait is agreed by both warps (bar.red.and) so that they leave
+// together.
+constexpr int ZP_WARPS = 4;  // warps per k_zpair CTA (two teams)
+
+// AND of v over the 64 threads of named barrier id (all must call).
+__device__ __forceinline__ bool team_and(bool v, int id) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 q, %1, 0;\n\t"
+      "bar.red.and.pred p, %2, 64, q;\n\t"
+      "selp.s32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"((int)v), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
+template <bool DA>
+__global__ void __launch_bounds__(ZP_WARPS * 32, ZW_MINB) k_zpair(ZCrossArgs<float> a) {
+  constexpr int H = 512, NTEAM = ZP_WARPS / 2;
+  using Z = ZW<H>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bars[NTEAM];
+  float2* tws = reinterpret_cast<float2*>(smem_raw);
+  const int Mz = DA ? zw_da_mz<H>() : a.Mz;
+  const int Mzp = DA ? (zw_da_mz<H>() + 7) / 8 * 8 : a.Mzp;
+  auto below = [](int k, int lo, int hi, int bound) { return hi < bound ? true : (lo >= bound ? false : k < bound); };
+  const int team = threadIdx.x >> 6, b = threadIdx.x & 63, lane = threadIdx.x & 31;
+  const int bar_id = 1 + team;
+  const ZwMid<H> mid(b);
+  const int stg_slots = 6 * Mzp;
+  float2* stg = tws + Z::TWS + team * (stg_slots + Z::XS);  // [field][Mzp]
+  float2* xch = stg + stg_slots;
+  const float2* twz = tws + Z::TWZ;
+  zw_fill_twiddles<H, ZP_WARPS * 32>(tws, a.tw);
+  const uint32_t mb = tma::smem_u32(&bars[team]);
+  if (b == 0) tma::mbar_init(mb, 1);
+  tma::fence_async_smem();
+  __syncthreads();
+
+  const int wait_limit = g_z_wait_limit;
+  const long long nteams = (long long)gridDim.x * NTEAM;
+  const uint32_t row_bytes = (uint32_t)(Mzp * sizeof(float2));
+  auto prefetch = [&](long long row) {  // the team's first warp issues the six row copies
+    if (b < 32) {
+      if (lane == 0) tma::mbar_expect_tx(mb, 6u * row_bytes);
+      __syncwarp();
+      if (lane < 6) tma::load_bytes(stg + lane * Mzp, a.buf + lane * a.c_stride + row * Mzp, row_bytes, mb);
+    }
+  };
+
+  pdl_wait();
+  pdl_trigger();
+  long long row = (long long)blockIdx.x * NTEAM + team;
+  if (row < a.nrows) prefetch(row);
+  uint32_t phase = 0;
+  const float s2 = 0.5f * a.scale * a.scale;  // both inverse normalisations and the r2c 1/2
+  for (; row < a.nrows; row += nteams) {
+    {
+      const bool mine = __all_sync(0xffffffffu, tma::mbar_wait(mb, phase, wait_limit));
+      const bool ok = team_and(mine, bar_id);
+      phase ^= 1;
+      if (!ok) {
+        if (b == 0) atomicExch(&g_z_timeout, 1);
+        tma::mbar_wait(mb, phase ^ 1, Z_WAIT);  // the copies in flight, once more with a limit
+        return;
+      }
+    }
+    float2 u0[8], u1[8], u2[8], n0[8], n1[8], n2[8];
+    float2 wz[8];  // e^{-2 pi i k / Nz} of this lane's positions k = b + 64 r
+#pragma unroll
+    for (int r = 0; r < 8; ++r) wz[r] = twz[b + Z::NB0 * r];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      const float2* srow = stg + c * Mzp;
+      float2 v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int k = b + Z::NB0 * r, kk = H - k;
+        float2 X = below(k, Z::NB0 * r, Z::NB0 * r + Z::NB0 - 1, Mz) ? srow[k] : make_float2(0.f, 0.f);
+        float2 Y = below(kk, H - Z::NB0 * r - Z::NB0 + 1, H - Z::NB0 * r, Mz) ? srow[kk] : make_float2(0.f, 0.f);
+        if (k == 0) {
+          X.y = 0.f;
+          Y.y = 0.f;
+        }
+        Y.y = -Y.y;
+        const float2 sm = cadd(X, Y), df = csub(X, Y);
+        float2 w = wz[r];
+        w.y = -w.y;
+        v[r] = cadd(sm, cmul_i(cmul(w, df)));
+      }
+      zw_transform<H, true>(v, xch, tws, b, mid, bar_id);
+      // the transform's first exchange barrier put both warps past their staged reads
+      if (c == 5 && row + nteams < a.nrows) prefetch(row + nteams);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const float2 x = v[r];
+        switch (c) {
+          case 0: u0[r] = x; break;
+          case 1: u1[r] = x; break;
+          case 2: u2[r] = x; break;
+          case 3:
+            n1[r] = __fmul2_rn(u2[r], x);
+            n2[r] = __fmul2_rn(u1[r], make_float2(-x.x, -x.y));
+            break;
+          case 4:
+            n0[r] = __fmul2_rn(u2[r], make_float2(-x.x, -x.y));
+            n2[r] = __ffma2_rn(u0[r], x, n2[r]);
+            break;
+          default:
+            n0[r] = __fmul2_rn(__ffma2_rn(u1[r], x, n0[r]), make_float2(s2, s2));
+            n1[r] = __fmul2_rn(__ffma2_rn(u0[r], make_float2(-x.x, -x.y), n1[r]), make_float2(s2, s2));
+            n2[r] = __fmul2_rn(n2[r], make_float2(s2, s2));
+            break;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = c == 0 ? n0[r] : (c == 1 ? n1[r] : n2[r]);
+      zw_transform<H, false>(v, xch, tws, b, mid, bar_id);
+      // Z[H - k] of k = b + 64 r: lane (64 - b) mod 64, value 7 - r; for b = 0
+      // this lane's own value (8 - r) mod 8 (Z[H] = Z[0])
+#pragma unroll
+      for (int r = 0; r < 8; ++r) xch[zw_slot<H>(b + Z::NB0 * r)] = v[r];
+      zw_sync<H>(bar_id);
+      const int pb = (Z::LPR - b) & (Z::LPR - 1);
+      float2 zb[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) zb[r] = b == 0 ? v[(8 - r) & 7] : xch[zw_slot<H>(pb + Z::NB0 * (7 - r))];
+      zw_sync<H>(bar_id);  // the exchange buffer is free for the next transform
+      float2* out = a.buf + c * a.c_stride + row * Mzp;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int k = b + Z::NB0 * r;
+        if (below(k, Z::NB0 * r, Z::NB0 * r + Z::NB0 - 1, Mzp)) {
+          float2 x = make_float2(0.f, 0.f);
+          if (below(k, Z::NB0 * r, Z::NB0 * r + Z::NB0 - 1, Mz)) {  // r2c_post with the 1/2 folded into s2
+            float2 bc = zb[r];
+            bc.y = -bc.y;
+            const float2 E = cadd(v[r], bc), O = cmul_mi(csub(v[r], bc));
+            x = cadd(E, cmul(wz[r], O));
+          }
+          out[k] = x;
+        }
+      }
+      // bin H (general path: Mz = H + 1) and the row padding past it
+      if (!DA && b < Mzp - H) {
+        float2 x = make_float2(0.f, 0.f);
+        if (b == 0 && H < Mz) {
+          float2 bc = v[0];
+          bc.y = -bc.y;
+          x = cadd(cadd(v[0], bc), cmul(twz[H], cmul_mi(csub(v[0], bc))));
+        }
+        out[H + b] = x;
+      }
+    }
+  }
+}
+
 // Plain z c2r / r2c (to_physical / to_spectral).  Persistent CTAs walk the
 // (component, RB-row group) pairs; the rows of the next group are staged with
 // cp.async while the current group is transformed (a warp per row), as in
@@ -714,11 +886,34 @@ template <int HH> cudaError_t launch_zwarp(const ZCrossArgs<float>& a, cudaStrea
   return da ? launch_zwarp_v<HH, true>(a, st) : launch_zwarp_v<HH, false>(a, st);
 }
 
-// float32 rows of Nz = 128, 256, 512 (whole row groups, staging rows of at
-// most H + 8 entries) take the warp-resident kernel; every other case k_zcross.
+template <bool DA> cudaError_t launch_zpair_v(const ZCrossArgs<float>& a, cudaStream_t st) {
+  static PerDevice ready, cache;
+  using Z = ZW<512>;
+  constexpr int NTEAM = ZP_WARPS / 2;
+  auto smem_of = [](int Mzp) { return sizeof(float2) * (Z::TWS + (size_t)NTEAM * (6 * Mzp + Z::XS)); };
+  const size_t smax = smem_of(512 + 8);  // the opt-in covers the largest staging rows
+  cudaError_t e = once_per_device(ready, [&] {
+    cudaError_t r = cudaFuncSetAttribute(k_zpair<DA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+    if (r != cudaSuccess) return r;
+    return cudaFuncSetAttribute(k_zpair<DA>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
+  });
+  if (e != cudaSuccess) return e;
+  const int nb = resident_grid(k_zpair<DA>, ZP_WARPS * 32, smax, (a.nrows + NTEAM - 1) / NTEAM, cache);
+  return launch_pdl(k_zpair<DA>, nb, ZP_WARPS * 32, smem_of(a.Mzp), st, a);
+}
+
+cudaError_t launch_zpair(const ZCrossArgs<float>& a, cudaStream_t st) {
+  const bool da = a.Mz == zw_da_mz<512>() && a.Mzp == (zw_da_mz<512>() + 7) / 8 * 8;
+  return da ? launch_zpair_v<true>(a, st) : launch_zpair_v<false>(a, st);
+}
+
+// float32 rows of Nz = 128 ... 1024 (whole row groups, staging rows of at most
+// H + 8 entries) take the warp-resident kernels (a warp pair per row at Nz =
+// 1024); every other case k_zcross.
 template <typename T> bool use_zwarp(int H, const ZCrossArgs<T>& a) {
-  if (!std::is_same<T, float>::value || !(H == 64 || H == 128 || H == 256)) return false;
-  const int rows = 256 / H;
+  if (!std::is_same<T, float>::value || !(H == 64 || H == 128 || H == 256 || H == 512)) return false;
+  const int rows = H <= 256 ? 256 / H : 1;
   return a.nrows % rows == 0 && a.Mzp % 8 == 0 && a.Mzp <= H + 8 && a.Mz <= a.Mzp;
 }
 
@@ -727,7 +922,8 @@ template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, c
     if (use_zwarp(H, a)) {
       if (H == 64) return launch_zwarp<64>(a, st);
       if (H == 128) return launch_zwarp<128>(a, st);
-      return launch_zwarp<256>(a, st);
+      if (H == 256) return launch_zwarp<256>(a, st);
+      return launch_zpair(a, st);
     }
   }
   return dispatch_half(H, [&](auto hh) {

@@ -1,14 +1,18 @@
 // Warp-resident transforms of the fused z pass (float32, H = Nz/2 in {64, 128,
-// 256}).
+// 256, 512}).
 //
-// A warp owns ROWS = 256/H whole (x, y) rows; LPR = H/8 lanes serve one row.
+// For H <= 256 a warp owns ROWS = 256/H whole (x, y) rows; LPR = H/8 lanes
+// serve one row.  For H = 512 a row needs LPR = 64 lanes: a team of two warps
+// owns it, and the team's exchanges are ordered by a named barrier over its 64
+// threads instead of __syncwarp (zw_sync).
 // The half-length complex transform of a row (H points, see k_z.cu) runs on
 // the plan radix 8 -> R1 -> radix 8 (R1 = H/64; H = 64 has no middle stage):
 // every stage leaves each lane holding 8 complex values, the radix-8 stages
 // one butterfly per lane, the middle stage 8/R1 butterflies per lane.  Values
-// move between stages through a warp-private shared exchange buffer, laid out
+// move between stages through a row-private shared exchange buffer, laid out
 // so that every access of a half warp hits 16 distinct bank pairs (zw_slot),
-// and ordered by __syncwarp: no CTA barrier anywhere in the row loop.
+// and ordered by __syncwarp (or the team barrier): no CTA barrier anywhere in
+// the row loop.
 //
 // The first stage of the plan reads positions b + (H/8) r of the lane's row
 // (b = lane % LPR, r = 0..7) and the last stage writes positions b + (H/8) r,
@@ -16,7 +20,9 @@
 // of all six fields: the cross product u x w is formed in registers, and the
 // product is already laid out as the forward transform's first-stage input.
 // The r2c post-processing pairs Z[k] with Z[H-k], which sits in lane
-// (LPR - b) mod LPR of the same row: one __shfl_sync per value.
+// (LPR - b) mod LPR of the same row: one __shfl_sync per value (H <= 256), or
+// a trip through the exchange buffer when the partner is in the other warp of
+// the team (H = 512).
 #pragma once
 
 #include "fft_core.cuh"
@@ -24,9 +30,10 @@
 namespace hit {
 
 template <int H> struct ZW {
-  static_assert(H == 64 || H == 128 || H == 256, "warp-resident z rows need H in {64, 128, 256}");
-  static constexpr int LPR = H / 8;      // lanes per row
-  static constexpr int ROWS = 32 / LPR;  // rows per warp
+  static_assert(H == 64 || H == 128 || H == 256 || H == 512, "warp-resident z rows need H in {64, ..., 512}");
+  static constexpr int LPR = H / 8;                 // lanes per row
+  static constexpr int TEAM = H <= 256 ? 1 : 2;     // warps per row
+  static constexpr int ROWS = H <= 256 ? 32 / LPR : 1;  // rows per warp (per team of two at H = 512)
   static constexpr int R1 = H / 64;      // middle radix (1: no middle stage)
   static constexpr int NB0 = H / 8;      // butterflies of a radix-8 stage
   static constexpr int XS = H == 64 ? H + H / 8 : H + H / 16;  // exchange slots per row (see zw_slot)
@@ -39,7 +46,7 @@ template <int H> struct ZW {
 };
 
 // Exchange slot of row position p: one pad slot after every 8 positions (H =
-// 64) or every 16 (H = 128, 256).  The accesses are, per half warp: the first
+// 64) or every 16 (H = 128, 256, 512).  The accesses are, per half warp: the first
 // stage's stores of positions 8b + r (16 consecutive b), the middle stage's
 // loads of contiguous runs and stores of two runs of 8 positions, the last
 // stage's loads of contiguous runs.  An 8-byte slot s uses the bank pair of s
@@ -84,6 +91,17 @@ __device__ const unsigned char kZwMid256[64] = {
     20, 21, 28, 29, 30, 31, 47, 52, 56, 57, 7,  11, 12, 16, 32, 33, 34, 35, 36, 43, 44, 45,
     46, 53, 54, 55, 22, 23, 24, 25, 26, 27, 48, 49, 50, 51, 58, 59, 60, 61, 62, 63};
 
+// Orders the exchange-buffer accesses of the threads that share a row: the
+// warp for H <= 256, the team's two warps (named barrier `id`, 64 threads) for
+// H = 512.
+template <int H> __device__ __forceinline__ void zw_sync(int id) {
+  if constexpr (ZW<H>::TEAM == 1) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory");
+  }
+}
+
 template <int H> struct ZwMid {
   static constexpr int R1 = ZW<H>::R1, C1 = R1 > 1 ? 8 / R1 : 1;
   int k[C1];   // twiddle index b1 % 8
@@ -106,16 +124,16 @@ template <int H> struct ZwMid {
 // The three stages of one H-point transform (INV: exp(+2 pi i nk/H)).  On
 // entry v[r] holds position b + (H/8) r of the lane's row, on exit output
 // b + (H/8) r.  xch is the row's exchange buffer; mid the lane's middle-stage
-// butterflies; the warp must call this converged.  Returns with the exchange
-// buffer free for the next transform.
+// butterflies; the warp (the team at H = 512, barrier bar_id) must call this
+// converged.  Returns with the exchange buffer free for the next transform.
 template <int H, bool INV>
 __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const float2* __restrict__ tws, int b,
-                                             const ZwMid<H>& mid) {
+                                             const ZwMid<H>& mid, int bar_id = 0) {
   using Z = ZW<H>;
   DFT<8, INV, float2>::run(v);  // stage 0 (P = 1): outputs 8b + r
 #pragma unroll
   for (int r = 0; r < 8; ++r) xch[zw_slot<H>(8 * b + r)] = v[r];
-  __syncwarp();
+  zw_sync<H>(bar_id);
   if constexpr (Z::R1 > 1) {
     constexpr int R1 = Z::R1, NB1 = H / R1, C1 = 8 / R1;
     float2 u[C1][R1];
@@ -125,7 +143,7 @@ __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const 
 #pragma unroll
       for (int r = 0; r < R1; ++r) u[i][r] = xch[mid.ld[i] + zw_slot<H>(NB1 * r)];
     }
-    __syncwarp();
+    zw_sync<H>(bar_id);
 #pragma unroll
     for (int i = 0; i < C1; ++i) {
       const int k = mid.k[i];
@@ -139,12 +157,12 @@ __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const 
 #pragma unroll
       for (int r = 0; r < R1; ++r) xch[mid.st[i] + zw_slot<H>(8 * r)] = u[i][r];
     }
-    __syncwarp();
+    zw_sync<H>(bar_id);
   }
   // last stage: radix 8, P = H/8, butterfly b (k = b, outputs b + (H/8) r)
 #pragma unroll
   for (int r = 0; r < 8; ++r) v[r] = xch[zw_slot<H>(b + Z::NB0 * r)];
-  __syncwarp();
+  zw_sync<H>(bar_id);
 #pragma unroll
   for (int r = 1; r < 8; ++r) {
     float2 w = tws[Z::TW2 + (r - 1) * Z::NB0 + b];
