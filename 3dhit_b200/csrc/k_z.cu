@@ -382,6 +382,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = lane / Z::LPR, b = lane % Z::LPR;
   const ZwMid<H> mid(b);
+  float2 wl[7];  // filled once the twiddle tables are in shared memory
   const int stg_slots = 6 * Z::ROWS * Mzp;
   float2* stg = tws + Z::TWS + warp * (stg_slots + Z::ROWS * Z::XS);  // [field][row][Mzp]
   float2* xch = stg + stg_slots + q * Z::XS;
@@ -391,6 +392,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
   if (lane == 0) tma::mbar_init(mb, 1);
   tma::fence_async_smem();
   __syncthreads();
+  zw_last_twiddles<H>(wl, tws, b);
 
   const int wait_limit = g_z_wait_limit;
   const long long ngroups = a.nrows / Z::ROWS;
@@ -422,12 +424,10 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
       }
     }
     float2 u0[8], u1[8], u2[8], n0[8], n1[8], n2[8];
-    // e^{-2 pi i k / Nz} of this lane's positions k = b + (H/8) r, loaded once
-    // for the pre-processing of the six fields and the post-processing of the
-    // three products
-    float2 wz[8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) wz[r] = twz[b + Z::NB0 * r];
+    // e^{-2 pi i k / Nz} of this lane's positions k = b + (H/8) r (zw_wz(wz0,
+    // r)) for the pre-processing of the six fields and the post-processing of
+    // the three products
+    const float2 wz0 = twz[b];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       // c2r pre-processing of positions k = b + (H/8) r (see c2r_pre)
@@ -444,11 +444,11 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
         }
         Y.y = -Y.y;
         const float2 sm = cadd(X, Y), df = csub(X, Y);
-        float2 w = wz[r];
+        float2 w = zw_wz(wz0, r);
         w.y = -w.y;
         v[r] = cadd(sm, cmul_i(cmul(w, df)));
       }
-      zw_transform<H, true>(v, xch, tws, b, mid);
+      zw_transform<H, true>(v, xch, tws, b, mid, wl);
       if (c == 5 && grp + nwarps < ngroups) prefetch(grp + nwarps);  // every lane is past its staged reads
       // u x w (navierstokes.py:82-86) in the packed form of the real rows:
       // n0 = u1 w2 - u2 w1, n1 = u2 w0 - u0 w2, n2 = u0 w1 - u1 w0
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
       float2 v[8];
 #pragma unroll
       for (int r = 0; r < 8; ++r) v[r] = c == 0 ? n0[r] : (c == 1 ? n1[r] : n2[r]);
-      zw_transform<H, false>(v, xch, tws, b, mid);
+      zw_transform<H, false>(v, xch, tws, b, mid, wl);
       float2* out = a.buf + c * a.c_stride + (grp * Z::ROWS + q) * Mzp;
       const int partner = q * Z::LPR + ((Z::LPR - b) & (Z::LPR - 1));
 #pragma unroll
@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
             float2 bc = zb;
             bc.y = -bc.y;
             const float2 E = cadd(v[r], bc), O = cmul_mi(csub(v[r], bc));
-            x = cadd(E, cmul(wz[r], O));
+            x = cadd(E, cmul(zw_wz(wz0, r), O));
           }
           out[k] = x;
         }
@@ -558,6 +558,7 @@ __global__ void __launch_bounds__(ZP_WARPS * 32, ZW_MINB) k_zpair(ZCrossArgs<flo
   const int team = threadIdx.x >> 6, b = threadIdx.x & 63, lane = threadIdx.x & 31;
   const int bar_id = 1 + team;
   const ZwMid<H> mid(b);
+  float2 wl[7];  // filled once the twiddle tables are in shared memory
   const int stg_slots = 6 * Mzp;
   float2* stg = tws + Z::TWS + team * (stg_slots + Z::XS);  // [field][Mzp]
   float2* xch = stg + stg_slots;
@@ -567,6 +568,7 @@ __global__ void __launch_bounds__(ZP_WARPS * 32, ZW_MINB) k_zpair(ZCrossArgs<flo
   if (b == 0) tma::mbar_init(mb, 1);
   tma::fence_async_smem();
   __syncthreads();
+  zw_last_twiddles<H>(wl, tws, b);
 
   const int wait_limit = g_z_wait_limit;
   const long long nteams = (long long)gridDim.x * NTEAM;
@@ -597,9 +599,7 @@ __global__ void __launch_bounds__(ZP_WARPS * 32, ZW_MINB) k_zpair(ZCrossArgs<flo
       }
     }
     float2 u0[8], u1[8], u2[8], n0[8], n1[8], n2[8];
-    float2 wz[8];  // e^{-2 pi i k / Nz} of this lane's positions k = b + 64 r
-#pragma unroll
-    for (int r = 0; r < 8; ++r) wz[r] = twz[b + Z::NB0 * r];
+    const float2 wz0 = twz[b];  // e^{-2 pi i k / Nz} of positions k = b + 64 r: zw_wz(wz0, r)
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       const float2* srow = stg + c * Mzp;
@@ -615,11 +615,11 @@ __global__ void __launch_bounds__(ZP_WARPS * 32, ZW_MINB) k_zpair(ZCrossArgs<flo
         }
         Y.y = -Y.y;
         const float2 sm = cadd(X, Y), df = csub(X, Y);
-        float2 w = wz[r];
+        float2 w = zw_wz(wz0, r);
         w.y = -w.y;
         v[r] = cadd(sm, cmul_i(cmul(w, df)));
       }
-      zw_transform<H, true>(v, xch, tws, b, mid, bar_id);
+      zw_transform<H, true>(v, xch, tws, b, mid, wl, bar_id);
       // the transform's first exchange barrier put both warps past their staged reads
       if (c == 5 && row + nteams < a.nrows) prefetch(row + nteams);
 #pragma unroll
@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(ZP_WARPS * 32, ZW_MINB) k_zpair(ZCrossArgs<flo
       float2 v[8];
 #pragma unroll
       for (int r = 0; r < 8; ++r) v[r] = c == 0 ? n0[r] : (c == 1 ? n1[r] : n2[r]);
-      zw_transform<H, false>(v, xch, tws, b, mid, bar_id);
+      zw_transform<H, false>(v, xch, tws, b, mid, wl, bar_id);
       // Z[H - k] of k = b + 64 r: lane (64 - b) mod 64, value 7 - r; for b = 0
       // this lane's own value (8 - r) mod 8 (Z[H] = Z[0])
 #pragma unroll
@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(ZP_WARPS * 32, ZW_MINB) k_zpair(ZCrossArgs<flo
             float2 bc = zb[r];
             bc.y = -bc.y;
             const float2 E = cadd(v[r], bc), O = cmul_mi(csub(v[r], bc));
-            x = cadd(E, cmul(wz[r], O));
+            x = cadd(E, cmul(zw_wz(wz0, r), O));
           }
           out[k] = x;
         }

@@ -102,18 +102,32 @@ template <int H> __device__ __forceinline__ void zw_sync(int id) {
   }
 }
 
+// H = 512 (one radix-8 middle butterfly per lane of a two-warp team): with
+// b1 = b the stores j + 8 r (j = 64 (b1 / 8) + b1 % 8) of a half warp put two
+// lanes on 4 of the bank pairs.  The same construction as for H = 256 -- four
+// perfect matchings of the 4-regular bipartite graph joining load bank pair
+// (b1 + b1 / 16) mod 16 to store bank pair (b1 % 8 + 4 (b1 / 8)) mod 16 --
+// gives each half warp of the team 16 butterflies whose loads and stores all
+// hit distinct bank pairs.  Entry [team lane].
+__device__ const unsigned char kZwMid512[64] = {
+    0,  1,  2,  3,  4,  9,  10, 11, 12, 13, 14, 15, 20, 21, 22, 23, 5,  6,  7,  8,  16, 17,
+    18, 19, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 41, 42, 43, 44, 45, 46, 47,
+    52, 53, 54, 55, 37, 38, 39, 40, 48, 49, 50, 51, 56, 57, 58, 59, 60, 61, 62, 63};
+
 template <int H> struct ZwMid {
   static constexpr int R1 = ZW<H>::R1, C1 = R1 > 1 ? 8 / R1 : 1;
   int k[C1];   // twiddle index b1 % 8
   int ld[C1];  // exchange slot of input b1 (input r at ld + zw_slot(r H / R1))
   int st[C1];  // exchange slot of output j (output r at st + zw_slot(8 r))
-  // once per thread (a load of the table at H = 256).  The offsets are
+  // once per thread (a load of the table at H = 256, 512).  The offsets are
   // additive: H / R1 = 64 is a multiple of 16, and j % 16 = b1 % 8 leaves
   // room for 8 r % 16 below 16.
   __device__ __forceinline__ explicit ZwMid(int b) {
 #pragma unroll
     for (int i = 0; i < C1; ++i) {
-      const int b1 = H == 256 ? (int)kZwMid256[32 * i + b] : b + ZW<H>::LPR * i;
+      const int b1 = H == 256   ? (int)kZwMid256[32 * i + b]
+                     : H == 512 ? (int)kZwMid512[b]
+                                : b + ZW<H>::LPR * i;
       k[i] = b1 & 7;
       ld[i] = zw_slot<H>(b1);
       st[i] = zw_slot<H>((b1 - k[i]) * R1 + k[i]);
@@ -128,7 +142,7 @@ template <int H> struct ZwMid {
 // converged.  Returns with the exchange buffer free for the next transform.
 template <int H, bool INV>
 __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const float2* __restrict__ tws, int b,
-                                             const ZwMid<H>& mid, int bar_id = 0) {
+                                             const ZwMid<H>& mid, const float2 (&wl)[7], int bar_id = 0) {
   using Z = ZW<H>;
   DFT<8, INV, float2>::run(v);  // stage 0 (P = 1): outputs 8b + r
 #pragma unroll
@@ -165,11 +179,34 @@ __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const 
   zw_sync<H>(bar_id);
 #pragma unroll
   for (int r = 1; r < 8; ++r) {
-    float2 w = tws[Z::TW2 + (r - 1) * Z::NB0 + b];
+    float2 w = wl[r - 1];
     if (INV) w.y = -w.y;
     v[r] = cmul(v[r], w);
   }
   DFT<8, INV, float2>::run(v);
+}
+
+// The last stage's twiddles w_H^{r b}, r = 1..7, of lane b: the same for every
+// row and transform the lane handles, so they are loaded once into registers
+// (the shared-memory loads they replace were an eighth of a row's exchange
+// traffic).
+template <int H> __device__ __forceinline__ void zw_last_twiddles(float2 (&wl)[7], const float2* tws, int b) {
+#pragma unroll
+  for (int r = 1; r < 8; ++r) wl[r - 1] = tws[ZW<H>::TW2 + (r - 1) * ZW<H>::NB0 + b];
+}
+
+// e^{-2 pi i k / (2H)} at k = b + (H/8) r from w0 = e^{-2 pi i b / (2H)}: the
+// step (H/8)/(2H) = 1/16 of a turn is the same for every H, so the factor is
+// w0 times e^{-i pi r / 8} (exact for r = 0 and 4).  This keeps one complex
+// value per lane instead of eight.  Called in fully unrolled loops, where r is
+// a constant and the selection folds away.
+__device__ __forceinline__ float2 zw_wz(float2 w0, int r) {
+  constexpr float c = 0.92387953251128675613f, s = 0.38268343236508977173f, h = 0.70710678118654752440f;
+  if (r == 0) return w0;
+  if (r == 4) return make_float2(w0.y, -w0.x);
+  const float cr = r == 1 ? c : r == 2 ? h : r == 3 ? s : r == 5 ? -s : r == 6 ? -h : -c;
+  const float ci = r == 1 ? -s : r == 2 ? -h : r == 3 ? -c : r == 5 ? -c : r == 6 ? -h : -s;
+  return cmul(w0, make_float2(cr, ci));
 }
 
 }  // namespace hit
