@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(128, 4) k_zles(ZLesArgs a) {
 }
 
 // k_zwarp: the fused z pass of k_zcross (same inputs, outputs and arithmetic
-// per value) with warp-resident transforms (zwarp.cuh), float32, H in {64,
+// per value) with warp-resident transforms (zwarp.cuh), float32, H in {32, 64,
 // 128, 256}.  Persistent CTAs of NWARP independent warps; warp g walks the row
 // groups g, g + (all warps), ...  A warp stages its group's 6 x ROWS input rows
 // (Mzp entries each) with bulk TMA copies issued by its lanes and counted on
@@ -401,9 +401,9 @@ __global__ void __launch_bounds__(NWARP * 32, ZW_MINB) k_zwarp(ZCrossArgs<float>
   auto prefetch = [&](long long grp) {
     if (lane == 0) tma::mbar_expect_tx(mb, 6u * Z::ROWS * row_bytes);
     __syncwarp();
-    if (lane < 6 * Z::ROWS) {  // lane = field * ROWS + row
-      const int c = lane / Z::ROWS, rr = lane % Z::ROWS;
-      tma::load_bytes(stg + lane * Mzp, a.buf + c * a.c_stride + (grp * Z::ROWS + rr) * Mzp, row_bytes, mb);
+    for (int i = lane; i < 6 * Z::ROWS; i += 32) {  // i = field * ROWS + row (48 rows at H = 32)
+      const int c = i / Z::ROWS, rr = i % Z::ROWS;
+      tma::load_bytes(stg + i * Mzp, a.buf + c * a.c_stride + (grp * Z::ROWS + rr) * Mzp, row_bytes, mb);
     }
   };
 
@@ -908,11 +908,11 @@ cudaError_t launch_zpair(const ZCrossArgs<float>& a, cudaStream_t st) {
   return da ? launch_zpair_v<true>(a, st) : launch_zpair_v<false>(a, st);
 }
 
-// float32 rows of Nz = 128 ... 1024 (whole row groups, staging rows of at most
+// float32 rows of Nz = 64 ... 1024 (whole row groups, staging rows of at most
 // H + 8 entries) take the warp-resident kernels (a warp pair per row at Nz =
 // 1024); every other case k_zcross.
 template <typename T> bool use_zwarp(int H, const ZCrossArgs<T>& a) {
-  if (!std::is_same<T, float>::value || !(H == 64 || H == 128 || H == 256 || H == 512)) return false;
+  if (!std::is_same<T, float>::value || !(H == 32 || H == 64 || H == 128 || H == 256 || H == 512)) return false;
   const int rows = H <= 256 ? 256 / H : 1;
   return a.nrows % rows == 0 && a.Mzp % 8 == 0 && a.Mzp <= H + 8 && a.Mz <= a.Mzp;
 }
@@ -920,6 +920,7 @@ template <typename T> bool use_zwarp(int H, const ZCrossArgs<T>& a) {
 template <typename T> cudaError_t launch_zcross(int H, const ZCrossArgs<T>& a, cudaStream_t st) {
   if constexpr (std::is_same<T, float>::value) {
     if (use_zwarp(H, a)) {
+      if (H == 32) return launch_zwarp<32>(a, st);
       if (H == 64) return launch_zwarp<64>(a, st);
       if (H == 128) return launch_zwarp<128>(a, st);
       if (H == 256) return launch_zwarp<256>(a, st);

@@ -1,12 +1,13 @@
-// Warp-resident transforms of the fused z pass (float32, H = Nz/2 in {64, 128,
-// 256, 512}).
+// Warp-resident transforms of the fused z pass (float32, H = Nz/2 in {32, 64,
+// 128, 256, 512}).
 //
 // For H <= 256 a warp owns ROWS = 256/H whole (x, y) rows; LPR = H/8 lanes
 // serve one row.  For H = 512 a row needs LPR = 64 lanes: a team of two warps
 // owns it, and the team's exchanges are ordered by a named barrier over its 64
 // threads instead of __syncwarp (zw_sync).
 // The half-length complex transform of a row (H points, see k_z.cu) runs on
-// the plan radix 8 -> R1 -> radix 8 (R1 = H/64; H = 64 has no middle stage):
+// the plan radix 8 -> R1 -> radix 8 (R1 = H/64; H = 64 has no middle stage;
+// H = 32 is radix 8 -> radix 4 with two radix-4 butterflies per lane):
 // every stage leaves each lane holding 8 complex values, the radix-8 stages
 // one butterfly per lane, the middle stage 8/R1 butterflies per lane.  Values
 // move between stages through a row-private shared exchange buffer, laid out
@@ -30,18 +31,23 @@
 namespace hit {
 
 template <int H> struct ZW {
-  static_assert(H == 64 || H == 128 || H == 256 || H == 512, "warp-resident z rows need H in {64, ..., 512}");
+  static_assert(H == 32 || H == 64 || H == 128 || H == 256 || H == 512,
+                "warp-resident z rows need H in {32, ..., 512}");
   static constexpr int LPR = H / 8;                 // lanes per row
   static constexpr int TEAM = H <= 256 ? 1 : 2;     // warps per row
   static constexpr int ROWS = H <= 256 ? 32 / LPR : 1;  // rows per warp (per team of two at H = 512)
   static constexpr int R1 = H / 64;      // middle radix (1: no middle stage)
   static constexpr int NB0 = H / 8;      // butterflies of a radix-8 stage
-  static constexpr int XS = H == 64 ? H + H / 8 : H + H / 16;  // exchange slots per row (see zw_slot)
+  static constexpr int XS = H <= 64 ? H + H / 8 : H + H / 16;  // exchange slots per row (see zw_slot)
+  // last stage: radix LR over stride LP (H = 32: two radix-4 butterflies per
+  // lane over P = 8; else one radix-8 butterfly per lane over P = H/8)
+  static constexpr int LR = H == 32 ? 4 : 8;
+  static constexpr int LP = H / LR;
   // twiddle tables: middle stage (R1-1) x 8, last stage 7 x H/8, then
   // exp(-2 pi i k / 2H) for k = 0..H (pre/post-processing of the real rows)
   static constexpr int TW1 = 0;
   static constexpr int TW2 = R1 > 1 ? (R1 - 1) * 8 : 0;
-  static constexpr int TWZ = TW2 + 7 * (H / 8);
+  static constexpr int TWZ = TW2 + (LR - 1) * LP;
   static constexpr int TWS = (TWZ + H + 1 + 1) / 2 * 2;  // even: what follows stays 16-byte aligned
 };
 
@@ -55,7 +61,7 @@ template <int H> struct ZW {
 // additive in the fields of p that a lane's index and a value's index r fill,
 // so every access is the lane's base slot plus a constant offset.
 template <int H> __device__ __forceinline__ int zw_slot(int p) {
-  return H == 64 ? p + (p >> 3) : p + (p >> 4);
+  return H <= 64 ? p + (p >> 3) : p + (p >> 4);
 }
 
 // Twiddle tables of ZW<H> from the global exp(-2 pi i m / TWN) table (all
@@ -67,8 +73,8 @@ template <int H, int NTH> __device__ __forceinline__ void zw_fill_twiddles(float
     if (e < Z::TW2) {  // middle stage: P = 8, radix R1: w_{8 R1}^{r k}
       const int r = e / 8 + 1, k = e % 8;
       m = r * k * (TWN / (8 * Z::R1));
-    } else if (e < Z::TWZ) {  // last stage: P = H/8, radix 8: w_H^{r k}
-      const int r = (e - Z::TW2) / Z::NB0 + 1, k = (e - Z::TW2) % Z::NB0;
+    } else if (e < Z::TWZ) {  // last stage: P = LP, radix LR: w_H^{r k}
+      const int r = (e - Z::TW2) / Z::LP + 1, k = (e - Z::TW2) % Z::LP;
       m = r * k * (TWN / H);
     } else if (e - Z::TWZ <= H) {
       m = (e - Z::TWZ) * (TWN / (2 * H));
@@ -144,6 +150,35 @@ template <int H, bool INV>
 __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const float2* __restrict__ tws, int b,
                                              const ZwMid<H>& mid, const float2 (&wl)[7], int bar_id = 0) {
   using Z = ZW<H>;
+  if constexpr (H == 32) {
+    // 8 x 4: stage 0 as below, then two radix-4 butterflies j = b + 4h (P = 8,
+    // inputs and outputs j + 8r), whose outputs b + 4 (h + 2r) are the lane's
+    // positions b + (H/8) r' with r' = h + 2r
+    DFT<8, INV, float2>::run(v);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) xch[zw_slot<H>(8 * b + r)] = v[r];
+    zw_sync<H>(bar_id);
+    float2 u[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) u[h][r] = xch[zw_slot<H>(b + 4 * h + 8 * r)];
+    }
+    zw_sync<H>(bar_id);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+      for (int r = 1; r < 4; ++r) {
+        float2 w = wl[3 * h + r - 1];
+        if (INV) w.y = -w.y;
+        u[h][r] = cmul(u[h][r], w);
+      }
+      DFT<4, INV, float2>::run(u[h]);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) v[h + 2 * r] = u[h][r];
+    }
+    return;
+  }
   DFT<8, INV, float2>::run(v);  // stage 0 (P = 1): outputs 8b + r
 #pragma unroll
   for (int r = 0; r < 8; ++r) xch[zw_slot<H>(8 * b + r)] = v[r];
@@ -191,8 +226,18 @@ __device__ __forceinline__ void zw_transform(float2 (&v)[8], float2* xch, const 
 // (the shared-memory loads they replace were an eighth of a row's exchange
 // traffic).
 template <int H> __device__ __forceinline__ void zw_last_twiddles(float2 (&wl)[7], const float2* tws, int b) {
+  using Z = ZW<H>;
+  if constexpr (H == 32) {  // w_32^{r j}, j = b + 4h, at wl[3h + r - 1]
 #pragma unroll
-  for (int r = 1; r < 8; ++r) wl[r - 1] = tws[ZW<H>::TW2 + (r - 1) * ZW<H>::NB0 + b];
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+      for (int r = 1; r < 4; ++r) wl[3 * h + r - 1] = tws[Z::TW2 + (r - 1) * Z::LP + b + 4 * h];
+    }
+    wl[6] = make_float2(1.f, 0.f);
+  } else {
+#pragma unroll
+    for (int r = 1; r < 8; ++r) wl[r - 1] = tws[Z::TW2 + (r - 1) * Z::NB0 + b];
+  }
 }
 
 // e^{-2 pi i k / (2H)} at k = b + (H/8) r from w0 = e^{-2 pi i b / (2H)}: the
