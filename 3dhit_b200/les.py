@@ -491,13 +491,27 @@ def les_window_grad(step, u0, nsteps, loss_fn):
     return L, gsum, lam, states[-1]
 
 
-def train_a_posteriori(data, model, iters=40, window=64, lr=3e-4, clip=1.0, tau_relax=0.5, seed=0, log=None):
+def train_a_posteriori(data, model, iters=40, window=64, lr=3e-4, clip=1.0, tau_relax=0.5, seed=0, log=None,
+                       select_every=0, select_steps=2000, val_snapshots=1):
     """Fine-tune a closure through the LES itself: each iteration runs the LES
     for ``window`` steps from a filtered DNS snapshot (the hold-energy forcing
     of `run_les`) and takes an Adam step on the gradient of the squared
     log-error of the final LES spectrum (shells 1..k_c) against the
     time-averaged filtered DNS spectrum, from `les_window_grad`; gradients
-    are clipped to global norm ``clip``.  Returns the loss history."""
+    are clipped to global norm ``clip``.  Returns the loss history.
+
+    Model selection (``select_every`` > 0): the short windows only
+    approximate what matters, the spectrum of a long LES run, and the
+    stochastic descent through a chaotic LES can leave weights that do well
+    on windows and drift on long runs.  The last ``val_snapshots`` snapshots
+    are then kept out of the windows; before the first iteration, every
+    ``select_every`` iterations and after the last, an LES of
+    ``select_steps`` steps from the last held-out snapshot is scored by its
+    maximum relative E(k) error (k <= k_c, samples after the first fifth)
+    against the time-averaged filtered DNS spectrum, and the weights with the
+    lowest score are restored at the end (the a-priori weights included).
+    The scores are left in ``model.a_posteriori_selection`` as (iteration,
+    score) pairs."""
     coarse = data["coarse"]
     kc = coarse.Nx // 3
     logT = torch.log(data["spectra"].mean(0)[:kc]).to(coarse.device)
@@ -510,8 +524,28 @@ def train_a_posteriori(data, model, iters=40, window=64, lr=3e-4, clip=1.0, tau_
     opt = torch.optim.Adam(model.params, lr=lr)
     gen = torch.Generator().manual_seed(seed)
     hist = []
+    ntrain = U.shape[0] - (val_snapshots if select_every > 0 else 0)
+    if ntrain < 1:
+        raise ValueError("no snapshots left for the windows after holding out the validation ones")
+    sel, best = [], None
+    ref = data["spectra"].mean(0)
+    val_data = dict(data, u0_coarse=U[-1])
+
+    def score(it):
+        nonlocal best
+        r = run_les(val_data, model, steps=select_steps, sample_every=50, discard=select_steps // 5,
+                    tau_relax=tau_relax)
+        sc = float((r["spectrum"] / ref - 1).abs().max()) if r["finite"] else float("inf")
+        sel.append((it, sc))
+        if best is None or sc < best[0]:
+            best = (sc, [q.detach().clone() for q in model.params])
+        if log:
+            log(f"a-posteriori selection at {it}: max E(k) error {sc:.4f}")
+
+    if select_every > 0:
+        score(0)
     for it in range(iters):
-        s = int(torch.randint(U.shape[0], (1,), generator=gen))
+        s = int(torch.randint(ntrain, (1,), generator=gen))
         step = FusedLESStep(coarse, model, p, dt)
         L, grads, _, _ = les_window_grad(step, U[s].clone(), window, lambda u: spectrum_log_loss(u, coarse, logT))
         norm = float(torch.sqrt(sum((d.double() ** 2).sum() for d in grads)))
@@ -524,6 +558,15 @@ def train_a_posteriori(data, model, iters=40, window=64, lr=3e-4, clip=1.0, tau_
         hist.append((it, s, L, norm))
         if log:
             log(f"a-posteriori {it}: snapshot {s}, loss {L:.4f}, |grad| {norm:.3g}")
+        if select_every > 0 and ((it + 1) % select_every == 0 or it + 1 == iters):
+            score(it + 1)
+    if best is not None:
+        with torch.no_grad():
+            for q, b in zip(model.params, best[1]):
+                q.copy_(b)
+        model._packed = None
+        model._physical = None
+    model.a_posteriori_selection = sel
     return hist
 
 

@@ -592,7 +592,8 @@ def run_closure(args):
     # a-posteriori tuning through the discrete adjoint of the LES
     t1 = time.perf_counter()
     apost = les.train_a_posteriori(data, model, iters=args.cl_apost_iters, window=args.cl_apost_window,
-                                   lr=args.cl_apost_lr, log=log)
+                                   lr=args.cl_apost_lr, log=log, select_every=args.cl_apost_select_every,
+                                   select_steps=args.cl_apost_select_steps)
     t_apost = time.perf_counter() - t1
     les_record("closure_a_posteriori", model, False)
     les_record("closure_a_posteriori_lagged", model, True)
@@ -610,6 +611,9 @@ def run_closure(args):
             "dns_ms_per_step": data["dns_ms_per_step"], "dns_dt": data["dt"], "mean_A": sum(data["A"]) / len(data["A"]),
             "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train, "a_posteriori": t_apost},
             "a_posteriori": {"iters": args.cl_apost_iters, "window": args.cl_apost_window, "lr": args.cl_apost_lr,
+                             "selection_every": args.cl_apost_select_every,
+                             "selection_steps": args.cl_apost_select_steps,
+                             "selection_max_err_Ek": getattr(model, "a_posteriori_selection", []),
                              "loss_first_last_10": [sum(h[2] for h in apost[:10]) / max(1, len(apost[:10])),
                                                     sum(h[2] for h in apost[-10:]) / max(1, len(apost[-10:]))]},
             **out}
@@ -658,6 +662,9 @@ def main():
     ap.add_argument("--cl-apost-iters", type=int, default=300)
     ap.add_argument("--cl-apost-window", type=int, default=64)
     ap.add_argument("--cl-apost-lr", type=float, default=3e-4)
+    ap.add_argument("--cl-apost-select-every", type=int, default=25,
+                    help="score the a-posteriori weights by a held-out LES every this many iterations, keep the best")
+    ap.add_argument("--cl-apost-select-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -40,3 +40,20 @@ def test_closure_beats_the_unmodelled_solver_and_adjoint_tuning_improves_it():
     assert prior[0] < none[0]
     assert cls_err < none[0]  # the classical closure removes the unmodelled solver's cut-off pile-up too
     assert post[0] < prior[0] and post[1] < prior[1]
+
+
+def test_a_posteriori_model_selection_keeps_the_best_scored_weights():
+    """With ``select_every`` the tuning scores the weights by a held-out LES
+    (before the first iteration, every few iterations and after the last)
+    and ends on the best-scored ones.  The LES is deterministic, so scoring
+    the final weights again reproduces the lowest recorded score exactly."""
+    data = les.make_dataset(fine_n=64, coarse_n=32, nu=4e-3, spinup=400, snapshots=12, every=25)
+    model, _ = les.train(data, steps=60, batch_snapshots=4, val_snapshots=2)
+    les.train_a_posteriori(data, model, iters=8, window=24, lr=3e-4, select_every=4, select_steps=400)
+    sel = model.a_posteriori_selection
+    assert [it for it, _ in sel] == [0, 4, 8]
+    ref = data["spectra"].mean(0)
+    r = les.run_les(dict(data, u0_coarse=data["U"][-1]), model, steps=400, sample_every=50, discard=80)
+    assert r["finite"]
+    again = float((r["spectrum"] / ref - 1).abs().max())
+    assert again == min(sc for _, sc in sel), (again, sel)
