@@ -506,7 +506,8 @@ def train_a_posteriori(data, model, iters=40, window=64, lr=3e-4, clip=1.0, tau_
     on windows and drift on long runs.  The last ``val_snapshots`` snapshots
     are then kept out of the windows; before the first iteration, every
     ``select_every`` iterations and after the last, an LES of
-    ``select_steps`` steps from the last held-out snapshot is scored by its
+    ``select_steps`` steps from the last held-out snapshot (time step from
+    that snapshot's CFL condition, as `run_les` forms it) is scored by its
     maximum relative E(k) error (k <= k_c, samples after the first fifth)
     against the time-averaged filtered DNS spectrum, and the weights with the
     lowest score are restored at the end (the a-priori weights included).
