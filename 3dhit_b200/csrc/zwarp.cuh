@@ -11,9 +11,10 @@
 // every stage leaves each lane holding 8 complex values, the radix-8 stages
 // one butterfly per lane, the middle stage 8/R1 butterflies per lane.  Values
 // move between stages through a row-private shared exchange buffer, laid out
-// so that every access of a half warp hits 16 distinct bank pairs (zw_slot),
-// and ordered by __syncwarp (or the team barrier): no CTA barrier anywhere in
-// the row loop.
+// so that every access of a half warp hits 16 distinct bank pairs (zw_slot;
+// the one exception is the middle stage's stores at H = 128, two-way on some
+// pairs), and ordered by __syncwarp (or the team barrier): no CTA barrier
+// anywhere in the row loop.
 //
 // The first stage of the plan reads positions b + (H/8) r of the lane's row
 // (b = lane % LPR, r = 0..7) and the last stage writes positions b + (H/8) r,
