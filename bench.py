@@ -19,6 +19,7 @@ Timing: W untimed warm-up steps, then K steps replayed from the CUDA graph,
 from __future__ import annotations
 
 import argparse
+import datetime
 import importlib
 import json
 import math
@@ -91,9 +92,13 @@ def kernel_alg_bytes(N, itemsize=8):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms, with the
+    sample times.  Started before the warm-up, so that nvidia-smi's own start
+    does not fall into the timed region; stop(t0, t1) keeps the samples taken
+    between the host times t0 and t1 that bracket the timed region (all of
+    them if none fall inside)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -107,7 +112,14 @@ class ClockSampler:
         except Exception:
             self.p = None
 
-    def stop(self):
+    @staticmethod
+    def _when(ts):
+        try:
+            return datetime.datetime.strptime(ts.strip(), "%Y/%m/%d %H:%M:%S.%f")
+        except ValueError:
+            return None
+
+    def stop(self, t0=None, t1=None):
         if self.p is None:
             return None
         self.p.terminate()
@@ -116,14 +128,18 @@ class ClockSampler:
         except Exception:
             self.p.kill()
         self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 9]
         os.unlink(self.f.name)
+        if t0 is not None and t1 is not None:
+            lo, hi = t0 - datetime.timedelta(seconds=0.2), t1 + datetime.timedelta(seconds=0.2)
+            inside = [r for r in rows if (w := self._when(r[0])) is not None and lo <= w <= hi]
+            rows = inside or rows
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = max(float(r[2]) for r in rows)
+        sm = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        mx = max(float(r[3]) for r in rows)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        reasons = sorted({n for r in rows for n, v in zip(names, r[6:10]) if "Active" in v and "Not" not in v})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
                 "samples": len(rows)}
 
@@ -625,7 +641,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=60)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--shape", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
@@ -688,8 +704,6 @@ def main():
     dev = torch.device("cuda", local)
     dist = None
     if world > 1:
-        import datetime
-
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
@@ -708,22 +722,25 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    # warm-up (captures the step graph)
+    # the clock sampler starts before the warm-up, so that nvidia-smi's start
+    # is over before the timed region; warm-up (captures the step graph)
+    clocks = ClockSampler(local) if rank == 0 else None
     u = h3.rollout(rhs, u0, p, dt, args.warmup, assume_dealiased=True, scheme=args.scheme)
     torch.cuda.synchronize()
 
     # ---- timed region: K graph-replayed steps ------------------------------
-    clocks = ClockSampler(local) if rank == 0 else None
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    t_wall0 = datetime.datetime.now()
     e0.record(stream)
     u = h3.rollout(rhs, u, p, dt, args.steps, assume_dealiased=True, scheme=args.scheme)
     e1.record(stream)
     torch.cuda.synchronize()
+    t_wall1 = datetime.datetime.now()
     barrier()
-    ck = clocks.stop() if clocks else None
+    ck = clocks.stop(t_wall0, t_wall1) if clocks else None
     ms_max = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     h3.check_device("bench timed rollout")  # no bounded wait of a transform pass gave up
     E_end = float(h3.energy(u, g))
