@@ -24,13 +24,15 @@ def test_transform_waits_never_gave_up(h3):
     assert st.value == 0
 
 
-def test_wait_give_up_is_reported_and_raised(h3):
+@pytest.mark.parametrize("dims", [(32, 32, 32), (16, 16, 512)])
+def test_wait_give_up_is_reported_and_raised(h3, dims):
     """With the wait limit at 0 polls every TMA tile wait gives up at once (the
-    CTA drains its copies with the default limit and ends): the device flag
-    is raised, `check_device` raises, and with the default limit restored the
+    CTA drains its copies with the default limit and ends; the 16 x 16 x 512
+    grid takes the warp-resident z pass of the 512^3 rows): the device flag is
+    raised, `check_device` raises, and with the default limit restored the
     same RHS is bit-identical to the one computed before."""
     nat = h3._native
-    g = h3.make_grid(32)
+    g = h3.make_grid(*dims)
     u0 = h3.hit_initial_field(0, g)
     p = h3.NSParams(nu=0.01, forcing=h3.BandForcing(eps=0.1, kmin=1.0, kmax=2.0))
     rhs = h3.make_ns_rhs(g)
