@@ -588,6 +588,7 @@ def run_closure(args):
 
     def les_record(name, cl, lag, fused=False):
         r = les.run_les(data, cl, steps=args.cl_les_steps, discard=args.cl_les_steps // 5, lag=lag,
+                        tau_relax=args.cl_tau,
                         fused_closure=fused)
         rel = (r["spectrum"] / ref - 1).abs()
         T = args.cl_les_steps * r["dt"]
@@ -601,13 +602,15 @@ def run_closure(args):
     for name, cl, lag in (("no_closure", None, False), ("closure", model, False), ("closure_lagged", model, True)):
         les_record(name, cl, lag)
     # the classical method without a network: Chollet-Lesieur spectral eddy viscosity
-    cl_spec = les.run_spectral_eddy_viscosity_les(data, args.cl_les_steps, args.cl_les_steps // 5)
+    cl_spec = les.run_spectral_eddy_viscosity_les(data, args.cl_les_steps, args.cl_les_steps // 5,
+                                                  tau_relax=args.cl_tau)
     out["chollet_lesieur"] = {"max_rel_err_Ek": float((cl_spec / ref - 1).abs().max()),
                               "mean_rel_err_Ek": float((cl_spec / ref - 1).abs().mean()),
                               "ratio_Ek": [round(float(x), 4) for x in cl_spec / ref]}
     # a-posteriori tuning through the discrete adjoint of the LES
     t1 = time.perf_counter()
     apost = les.train_a_posteriori(data, model, iters=args.cl_apost_iters, window=args.cl_apost_window,
+                                   tau_relax=args.cl_tau,
                                    lr=args.cl_apost_lr, log=log, select_every=args.cl_apost_select_every,
                                    select_steps=args.cl_apost_select_steps)
     t_apost = time.perf_counter() - t1
@@ -622,7 +625,7 @@ def run_closure(args):
                                    f"{args.cl_spinup} spin-up steps, {args.cl_snapshots} snapshots every "
                                    f"{args.cl_every} steps, filter k_c={kc}; MLP 9->64->64->64->6 GELU bf16; "
                                    f"LES {args.cl_les_steps} steps, Lundgren forcing holding the filtered DNS energy "
-                                   f"(relaxation 0.5); SGS stress once per RK4 step; closure rescaled to the DNS SGS "
+                                   f"(relaxation {args.cl_tau}); SGS stress once per RK4 step; closure rescaled to the DNS SGS "
                                    f"energy transfer"},
             "dns_ms_per_step": data["dns_ms_per_step"], "dns_dt": data["dt"], "mean_A": sum(data["A"]) / len(data["A"]),
             "train_loss_history": hist, "seconds": {"data": t_data, "train": t_train, "a_posteriori": t_apost},
@@ -681,6 +684,9 @@ def main():
     ap.add_argument("--cl-apost-select-every", type=int, default=25,
                     help="score the a-posteriori weights by a held-out LES every this many iterations, keep the best")
     ap.add_argument("--cl-apost-select-steps", type=int, default=2000)
+    ap.add_argument("--cl-tau", type=float, default=0.05,
+                    help="relaxation time of the LES's hold-energy forcing (training windows and LES runs); "
+                         "its steady state sits tau x (SGS transfer) below the filtered DNS energy")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
