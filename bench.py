@@ -678,7 +678,7 @@ def main():
     ap.add_argument("--cl-every", type=int, default=50)
     ap.add_argument("--cl-train-steps", type=int, default=400)
     ap.add_argument("--cl-les-steps", type=int, default=5000)
-    ap.add_argument("--cl-apost-iters", type=int, default=300)
+    ap.add_argument("--cl-apost-iters", type=int, default=600)
     ap.add_argument("--cl-apost-window", type=int, default=64)
     ap.add_argument("--cl-apost-lr", type=float, default=3e-4)
     ap.add_argument("--cl-apost-select-every", type=int, default=25,
