@@ -44,7 +44,7 @@ template <int H> struct ZW {
   // lane over P = 8; else one radix-8 butterfly per lane over P = H/8)
   static constexpr int LR = H == 32 ? 4 : 8;
   static constexpr int LP = H / LR;
-  // twiddle tables: middle stage (R1-1) x 8, last stage 7 x H/8, then
+  // twiddle tables: middle stage (R1-1) x 8, last stage (LR-1) x LP, then
   // exp(-2 pi i k / 2H) for k = 0..H (pre/post-processing of the real rows)
   static constexpr int TW1 = 0;
   static constexpr int TW2 = R1 > 1 ? (R1 - 1) * 8 : 0;
@@ -53,14 +53,17 @@ template <int H> struct ZW {
 };
 
 // Exchange slot of row position p: one pad slot after every 8 positions (H =
-// 64) or every 16 (H = 128, 256, 512).  The accesses are, per half warp: the first
-// stage's stores of positions 8b + r (16 consecutive b), the middle stage's
-// loads of contiguous runs and stores of two runs of 8 positions, the last
-// stage's loads of contiguous runs.  An 8-byte slot s uses the bank pair of s
-// mod 16, and all of these accesses get 16 distinct pairs except the middle
-// stage's stores (two lanes per pair on half of them).  The padding is
-// additive in the fields of p that a lane's index and a value's index r fill,
-// so every access is the lane's base slot plus a constant offset.
+// 32, 64) or every 16 (H = 128, 256, 512).  The accesses are, per half warp:
+// the first stage's stores of positions 8b + r (16 consecutive b), the middle
+// stage's loads of contiguous runs and stores of two runs of 8 positions, the
+// last stage's loads of contiguous runs.  An 8-byte slot s uses the bank pair
+// of s mod 16, and all of these accesses get 16 distinct pairs except the
+// middle stage's stores with butterflies assigned in order (b1 = b + LPR i):
+// the tables below fix that at H = 256 and 512; at H = 128 the stores' pairs
+// take only 15 values over the 64 butterflies, so some stay two-way.  The
+// padding is additive in the fields of p that a lane's index and a value's
+// index r fill, so every access is the lane's base slot plus a constant
+// offset.
 template <int H> __device__ __forceinline__ int zw_slot(int p) {
   return H <= 64 ? p + (p >> 3) : p + (p >> 4);
 }
