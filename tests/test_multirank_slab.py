@@ -1,4 +1,4 @@
-"""Slab-decomposed RHS (3dhit_b200/slab.py) as two gloo ranks on the CPU:
+"""Slab-decomposed RHS (3dhit_b200/slab.py) as two and four gloo ranks on the CPU:
 the kx-slab / y-slab partition and its all-to-all exchanges, with the local
 per-axis transforms supplied here on torch.fft (the CUDA passes need a GPU),
 against the oracle's RHS on the whole state in float64.  Unmeasured on GPU
@@ -73,18 +73,19 @@ def _worker(rank, world, port, dims, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("dims", [(16, 16, 16), (16, 8, 32)])
-def test_two_rank_slab_rhs_matches_oracle(orc, dims):
-    world = 2
+# four ranks exercise the all-to-all's block order, which two ranks cannot
+# tell from its reverse
+@pytest.mark.parametrize("world,dims", [(2, (16, 16, 16)), (2, (16, 8, 32)), (4, (16, 8, 32))])
+def test_slab_rhs_matches_oracle(orc, world, dims):
     out = mp.Manager().dict()
     mp.start_processes(_worker, args=(world, _free_port(), dims, out), nprocs=world, start_method="spawn")
     og = orc.make_grid(*dims, dtype=np.float64)
     u = orc.hit_initial_field(0, og, k0=2.0)
-    assert out[0]["roundtrip"] and out[1]["roundtrip"]
+    assert all(out[r]["roundtrip"] for r in range(world))
     forcings = {"none": orc.NoForcing(), "linear": orc.LinearForcing(A=0.1333),
                 "band": orc.BandForcing(eps=0.1, kmin=1.0, kmax=2.0),
                 "hold": orc.HoldEnergyForcing(1.5, 0.02, tau=0.7)}
     for name, f in forcings.items():
         ref = orc.make_ns_rhs(og)(u, orc.NSParams(nu=0.02, forcing=f), 0.0)
-        got = np.concatenate([out[0][name], out[1][name]], axis=1)  # kx slabs in rank order
+        got = np.concatenate([out[r][name] for r in range(world)], axis=1)  # kx slabs in rank order
         assert rel_l2(got, ref) < 1e-12, name
